@@ -1,0 +1,191 @@
+/*
+ * sepgraph.h — C ABI of the B200-native hybrid graph engine (libsepgraph_b200.so).
+ *
+ * The reference (SEP-Graph) exposes its hot path as a header-only C++ template
+ * API: Engine<TValue,TBuffer,TWeight,TAppImpl,...> driven by the four sample
+ * functions HybridBFS/HybridSSSP/HybridPageRank/HybridBC.  Device functors
+ * cannot cross a C ABI, so the functor/template layer stays C++ (see
+ * sep-graph_b200/csrc/sg_api.cuh and sg_engine.cuh) and this ABI exposes the
+ * four instantiated algorithms plus the graph store, options and statistics.
+ * Each entry point names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every call returns an sg_status; nothing calls exit() or assert() (the
+ *    reference uses exit(1) in GROUTE_CUDA_CHECK, include/groute/internal/cuda_utils.h:41-65).
+ *  - Output buffers are caller-owned.  An output pointer may be host memory
+ *    (pageable or pinned) or device memory on the context's device; the
+ *    library detects which with cudaPointerGetAttributes.
+ *  - One sg_ctx per host thread.  All work of a context is ordered on its
+ *    stream (sg_ctx_set_stream to share a caller's stream).
+ *  - Indices are uint32 (index_t in include/groute/graphs/common.h:36);
+ *    edge counts are uint64 at the boundary and must be < 2^32 inside.
+ */
+#ifndef SEPGRAPH_B200_H
+#define SEPGRAPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_ABI_VERSION 1
+
+typedef enum sg_status {
+    SG_OK = 0,
+    SG_ERR_INVALID_ARG = 1,   /* null pointer, out-of-range vertex, bad option */
+    SG_ERR_CUDA = 2,          /* a CUDA runtime call failed (message in sg_last_error) */
+    SG_ERR_OUT_OF_MEMORY = 3, /* device or host allocation failed */
+    SG_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up (no GPU hang) */
+    SG_ERR_CAPACITY = 5,      /* a device worklist would have overflowed; nothing was written past it */
+    SG_ERR_UNSUPPORTED = 6,   /* variant the reference also rejects (e.g. ASYNC_PULL_TD, framework.cuh:672-673) */
+    SG_ERR_OVERFLOW = 7,      /* uint64 path count overflow in BC */
+    SG_ERR_NO_DEVICE = 8,     /* no CUDA device / cooperative launch unsupported */
+    SG_ERR_IO = 9,            /* graph file could not be read or written */
+    SG_ERR_FORMAT = 10,       /* graph file is malformed */
+    SG_ERR_BUSY = 11          /* server queue full / budget exhausted */
+} sg_status;
+
+typedef struct sg_ctx sg_ctx;             /* device + stream + scratch cache */
+typedef struct sg_graph sg_graph;         /* device-resident CSR (+CSC) graph */
+typedef struct sg_hgraph sg_hgraph;       /* host CSR graph (generators, file I/O) */
+
+/* ------------------------------------------------------------------ selectors
+ * Mirror of include/framework/common.h:13-41 (LoadBalancing, Priority, Model,
+ * MsgPassing, Scheduling) and AlgoVariant (common.h:43-177).  A variant id is
+ * (model << 2) | (msg_passing << 1) | scheduling with SYNC=0/ASYNC=1,
+ * PUSH=0/PULL=1, TOPOLOGY_DRIVEN=0/DATA_DRIVEN=1. */
+enum { SG_LB_NONE = 0, SG_LB_COARSE_GRAINED = 1, SG_LB_FINE_GRAINED = 2, SG_LB_HYBRID = 3, SG_LB_AUTO = -1 };
+enum { SG_PRIORITY_NONE = 0, SG_PRIORITY_LOW_HIGH = 1, SG_PRIORITY_SAMPLING = 2 };
+enum {
+    SG_VARIANT_AUTO = -1,
+    SG_SYNC_PUSH_TD = 0, SG_SYNC_PUSH_DD = 1, SG_SYNC_PULL_TD = 2, SG_SYNC_PULL_DD = 3,
+    SG_ASYNC_PUSH_TD = 4, SG_ASYNC_PUSH_DD = 5, SG_ASYNC_PULL_TD = 6, SG_ASYNC_PULL_DD = 7
+};
+
+/* Graph creation flags. */
+#define SG_GRAPH_SYMMETRIC 0x1u  /* CSC aliases CSR (reference --undirected, csr_graph.h:405-410) */
+#define SG_GRAPH_NO_CSC 0x2u     /* do not build the in-edge (CSC) view; pull variants then fail */
+
+/* Engine options: union of EngineOptions (common.h:203-321) and the flags the
+ * reference reads from gflags (include/utils/app_skeleton.h:42-87). */
+typedef struct sg_options {
+    int32_t variant;          /* SG_VARIANT_AUTO = hybrid policy; else ForceVariant() */
+    int32_t lb_push;          /* SetLoadBalancing(PUSH, ..); SG_LB_AUTO = --lb_push "" rule */
+    int32_t lb_pull;          /* SetLoadBalancing(PULL, ..) */
+    int32_t priority;         /* SG_PRIORITY_NONE / LOW_HIGH (SetTwoLevelBasedPriority) */
+    double priority_delta;    /* two-level priority step; <=0 with LOW_HIGH = auto (32*avg_w/avg_deg) */
+    double cut_threshold;     /* SetSampleBasedPriority (accepted, see DESIGN) */
+    double alpha;             /* --alpha (15) */
+    double beta;              /* --beta (18) */
+    double edge_factor;       /* --edge_factor (1.0) */
+    int32_t max_iteration;    /* --max_iteration (200) */
+    int32_t fused;            /* SetFused(); the device-resident round loop is always used */
+    int32_t block_size;       /* --block_size (256); 0 = library choice */
+    int32_t non_atomic;       /* BFS --non_atomic (true) */
+    int32_t trace;            /* --trace: record one sg_round_trace per round */
+    double pr_error;          /* PageRank residual threshold (--error, 0.01) */
+    double timeout_s;         /* bound on any device-side wait; 0 = default (30 s) */
+    int32_t blocking;         /* 1: wait and fill sg_stats (default); 0: enqueue only */
+    int32_t reserved[7];
+} sg_options;
+
+/* Per-round trace record (the reference's --trace line, framework.cuh:334-348). */
+typedef struct sg_round_trace {
+    uint32_t round;
+    int32_t variant;
+    uint32_t in_nodes, out_nodes;
+    uint64_t in_workload, out_workload;
+    int64_t total_workload;
+    float time_ms;
+    uint32_t pad;
+} sg_round_trace;
+
+/* Run statistics (RunningInfo, include/framework/hybrid_policy.h:36-120). */
+typedef struct sg_stats {
+    uint32_t rounds;               /* num_iteration */
+    uint32_t max_iteration_reached;
+    uint32_t rounds_by_variant[8]; /* indexed by variant id */
+    double time_total_ms;          /* device time of the whole solve (CUDA events) */
+    double time_kernel_ms;         /* device time of the round loop */
+    uint64_t edges_processed;      /* edges expanded or scanned, summed over rounds */
+    uint64_t vertices_processed;   /* worklist items processed, summed over rounds */
+    uint64_t edges_reached;        /* sum of out-degrees of reached vertices (GTEPS numerator) */
+    uint32_t vertices_reached;
+    uint32_t search_depth;         /* BFS/BC: max level */
+    uint32_t device_error;         /* raw device error bits (0 = none) */
+    uint32_t n_trace;              /* number of records written to trace (if provided) */
+    sg_round_trace *trace;         /* caller-provided array or NULL */
+    uint32_t trace_capacity;
+    uint32_t pad;
+} sg_stats;
+
+/* ------------------------------------------------------------------ context */
+const char *sg_status_string(sg_status s);
+int sg_abi_version(void);
+/* Replaces Engine::Engine(AlgoType)'s device setup (framework.cuh:84-93), which is hard-wired to device 0. */
+sg_status sg_init(int device, sg_ctx **out);
+sg_status sg_destroy(sg_ctx *ctx);
+sg_status sg_ctx_set_stream(sg_ctx *ctx, void *cuda_stream); /* NULL = context's own stream */
+sg_status sg_ctx_get_stream(sg_ctx *ctx, void **cuda_stream);
+/* Waits for all enqueued work; returns the first device error of non-blocking calls. */
+sg_status sg_ctx_synchronize(sg_ctx *ctx);
+/* Detail message of the last failure on this context (never NULL). */
+const char *sg_last_error(const sg_ctx *ctx);
+sg_status sg_device_info(sg_ctx *ctx, int *sm_count, uint64_t *hbm_bytes, uint64_t *l2_bytes, char *name, size_t name_len);
+
+/* ------------------------------------------------------------------ graph store
+ * Replaces Engine::LoadGraph (framework.cuh:99-133) + single::CSRGraphAllocator /
+ * CSCGraphAllocator (csr_graph.h:1596-1783): uploads CSR, builds CSC (csr_tocsc,
+ * csr_graph.h:329-397) unless symmetric. offsets has nv+1 entries. */
+sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
+                          const uint32_t *weights, uint32_t flags, sg_graph **out);
+sg_status sg_graph_create_from_host(sg_ctx *ctx, const sg_hgraph *h, uint32_t flags, sg_graph **out);
+sg_status sg_graph_destroy(sg_graph *g);
+sg_status sg_graph_info(const sg_graph *g, uint32_t *nv, uint64_t *ne, uint64_t *device_bytes, int *weighted);
+
+sg_status sg_options_default(sg_options *opt);
+
+/* ------------------------------------------------------------------ algorithms */
+/* HybridBFS (samples/hybrid_bfs/hybrid_bfs.cu:173-243). levels_out: nv uint32, UINT32_MAX = unreached. */
+sg_status sg_bfs(sg_graph *g, uint32_t source, const sg_options *opt, uint32_t *levels_out, sg_stats *stats);
+/* HybridSSSP (samples/hybrid_sssp/hybrid_sssp.cu:151-243). Unweighted graphs use weight 1. */
+sg_status sg_sssp(sg_graph *g, uint32_t source, const sg_options *opt, uint32_t *dist_out, sg_stats *stats);
+/* HybridPageRank (samples/hybrid_pr/hybrid_pr.cu:128-210). Damping 0.85 as ALPHA in hybrid_pr_common.h:39.
+ * ranks_out: nv float (the engine value array); residual_out optional (GatherBuffer). */
+sg_status sg_pagerank(sg_graph *g, const sg_options *opt, float *ranks_out, float *residual_out, sg_stats *stats);
+/* HybridBC (samples/hybrid_bc/hybrid_bc.cu:303-412): single-source Brandes, bc already halved
+ * like hybrid_bc.cu:374-376. sigma_out optional (uint64 path counts). */
+sg_status sg_bc(sg_graph *g, uint32_t source, const sg_options *opt, float *bc_out, uint64_t *sigma_out,
+                sg_stats *stats);
+
+/* ------------------------------------------------------------------ host graphs (ingest)
+ * Seeded generators (the reference's generators are unseeded, traversal.h:173-189)
+ * and Galois .gr I/O (src/utils/parser.cpp:409-506). */
+#define SG_GEN_SYMMETRIC 0x1u      /* add reverse edges (gtools-style symmetrise) */
+#define SG_GEN_KEEP_SELF_LOOPS 0x2u
+#define SG_GEN_KEEP_DUPLICATES 0x4u
+sg_status sg_hgraph_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
+                             uint32_t flags, sg_hgraph **out);
+sg_status sg_hgraph_gen_grid(uint32_t rows, uint32_t cols, uint32_t flags, sg_hgraph **out);
+sg_status sg_hgraph_from_csr(uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
+                             const uint32_t *weights, sg_hgraph **out);
+/* Attach uniform weights in [lo, hi) drawn from a counter-based stream (seed, edge index). */
+sg_status sg_hgraph_gen_weights(sg_hgraph *h, uint32_t lo, uint32_t hi, uint64_t seed);
+sg_status sg_hgraph_read_gr(const char *path, sg_hgraph **out);
+sg_status sg_hgraph_write_gr(const sg_hgraph *h, const char *path);
+sg_status sg_hgraph_read_market(const char *path, int symmetrize, sg_hgraph **out);
+/* Pointers stay valid until sg_hgraph_destroy. weights is NULL when unweighted. */
+sg_status sg_hgraph_info(const sg_hgraph *h, uint32_t *nv, uint64_t *ne, const uint32_t **offsets,
+                         const uint32_t **indices, const uint32_t **weights);
+/* GetMaxOutDgrNode (csr_graph.h:241-259): lowest id among maximum out-degree. */
+sg_status sg_hgraph_max_degree_vertex(const sg_hgraph *h, uint32_t *vertex, uint32_t *degree);
+/* n seeded random vertices with out-degree > 0. */
+sg_status sg_hgraph_pick_sources(const sg_hgraph *h, uint32_t n, uint64_t seed, uint32_t *out);
+sg_status sg_hgraph_destroy(sg_hgraph *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEPGRAPH_B200_H */

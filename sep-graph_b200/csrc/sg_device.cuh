@@ -1,0 +1,146 @@
+// Device primitives of the B200 hybrid engine: a bounded grid barrier whose
+// last arriving block runs a single-thread callback, warp-aggregated worklist
+// appends, bitmap frontier helpers and small warp collectives.
+//
+// Reference counterparts: cub::GridBarrier (unbounded spin, used by the fused
+// kernels in include/framework/variants/driver.cuh:533-685), dev::Queue::append
+// (one atomicAdd per item, include/groute/device/queue.cuh:84-88; its
+// warp-aggregated append_warp at 90-116 is unused), and CompressedBitmap
+// (64-bit words, CAS set_bit_atomic, include/groute/device/compressed_bitmap.cuh:35-48).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sepgraph {
+namespace dev {
+
+constexpr uint32_t kFullMask = 0xffffffffu;
+
+// Device error bits (reported through sg_stats.device_error and mapped to sg_status).
+enum : uint32_t {
+    kErrTimeout = 1u,        // a bounded wait gave up
+    kErrCapacity = 2u,       // a worklist reservation exceeded its capacity (nothing written past it)
+    kErrOverflow = 4u,       // uint64 path-count overflow (BC)
+    kErrUnsupported = 8u,    // variant not implemented (same set as the reference's assert(false))
+    kErrChunkCapacity = 16u  // heavy-vertex chunk table overflow
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t warp_id() { return threadIdx.x >> 5; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Loads of state that other blocks modify inside the same launch go through L2.
+template <typename T>
+__device__ __forceinline__ T ld_l2(const T *p) {
+    return __ldcg(p);
+}
+
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x) {
+    const uint32_t lane = lane_id();
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(kFullMask, x, d);
+        if (lane >= (uint32_t)d) x += y;
+    }
+    return x;
+}
+template <typename T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(kFullMask, x, d);
+    return x;
+}
+
+// Warp-aggregated append: one atomicAdd per warp, items packed in lane order.
+// Must be called by all 32 lanes.  A reservation past `cap` writes nothing and
+// raises kErrCapacity instead of the reference's silent out-of-bounds write
+// (queue.cuh:86 asserts only in debug builds).
+__device__ __forceinline__ uint32_t warp_append(uint32_t *queue, uint32_t *count, uint32_t cap, bool want,
+                                                uint32_t item, uint32_t *err) {
+    const uint32_t m = __ballot_sync(kFullMask, want);
+    if (m == 0) return 0;
+    const uint32_t leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+    base = __shfl_sync(kFullMask, base, leader);
+    if (want) {
+        const uint32_t pos = base + __popc(m & lanemask_lt());
+        if (pos < cap)
+            queue[pos] = item;
+        else
+            atomicOr(err, kErrCapacity);
+    }
+    return m;
+}
+
+__device__ __forceinline__ bool bitmap_test(const uint32_t *bm, uint32_t v) {
+    return (ld_l2(bm + (v >> 5)) >> (v & 31u)) & 1u;
+}
+// Returns true if this call set the bit.
+__device__ __forceinline__ bool bitmap_set(uint32_t *bm, uint32_t v) {
+    const uint32_t bit = 1u << (v & 31u);
+    return (atomicOr(bm + (v >> 5), bit) & bit) == 0;
+}
+__device__ __forceinline__ void bitmap_clear(uint32_t *bm, uint32_t v) { atomicAnd(bm + (v >> 5), ~(1u << (v & 31u))); }
+
+// Bounded grid barrier for a cooperative launch (all blocks co-resident).
+// The last block to arrive runs `leader()` on one thread with every block's
+// prior writes visible, then releases the others; its writes are visible to
+// all blocks after the barrier.  A waiter that exceeds timeout_ns raises
+// kErrTimeout and returns false instead of spinning forever; every block then
+// leaves the kernel at its next barrier or status check.
+template <typename Leader>
+__device__ __forceinline__ bool grid_barrier(uint32_t *bar_count, uint32_t *bar_gen, uint32_t *err,
+                                             uint64_t timeout_ns, Leader &&leader) {
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t ok = 1;
+        const uint32_t g = ld_acquire(bar_gen);
+        __threadfence();
+        const uint32_t arrived = atomicAdd(bar_count, 1u);
+        if (arrived == gridDim.x - 1) {
+            __threadfence();
+            *bar_count = 0;
+            leader();
+            __threadfence();
+            st_release(bar_gen, g + 1);
+        } else {
+            const uint64_t t0 = globaltimer_ns();
+            uint32_t spins = 0;
+            while (ld_acquire(bar_gen) == g) {
+                ++spins;
+                if ((spins & 255u) == 0 && (globaltimer_ns() - t0 > timeout_ns || spins > (1u << 28))) {
+                    atomicOr(err, kErrTimeout);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        if (ld_l2(err) & kErrTimeout) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+}  // namespace dev
+}  // namespace sepgraph

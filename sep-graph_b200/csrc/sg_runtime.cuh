@@ -1,0 +1,376 @@
+// Host runtime of the B200 hybrid engine: context, device graph store,
+// per-graph workspace cache, the cooperative launch of the engine kernel and
+// the C++ Engine class that mirrors the reference's
+// sepgraph::engine::Engine (include/framework/framework.cuh:56-797).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/sepgraph.h"
+#include "sg_engine.cuh"
+
+struct sg_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaDeviceProp prop{};
+    std::string last_error;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t pending_error = 0;
+    // pinned host staging for control-block read-back
+    void *pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+namespace sgb {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+// Grow-only device buffers owned by one graph.  Work on a context is ordered
+// on its stream, so consecutive queries reuse them without reallocating.
+struct Workspace {
+    std::map<std::string, DevBuf> bufs;
+    ~Workspace() {
+        for (auto &kv : bufs)
+            if (kv.second.p) cudaFree(kv.second.p);
+    }
+    template <typename T>
+    cudaError_t get(const char *name, size_t count, T **out, bool zero_new = false) {
+        DevBuf &b = bufs[name];
+        size_t bytes = count * sizeof(T);
+        if (bytes == 0) bytes = 256;
+        bytes = (bytes + 255) & ~size_t(255);
+        if (b.bytes < bytes) {
+            if (b.p) cudaFree(b.p);
+            b.p = nullptr;
+            b.bytes = 0;
+            cudaError_t e = cudaMalloc(&b.p, bytes);
+            if (e != cudaSuccess) return e;
+            b.bytes = bytes;
+            if (zero_new) {
+                e = cudaMemset(b.p, 0, bytes);
+                if (e != cudaSuccess) return e;
+            }
+        }
+        *out = (T *)b.p;
+        return cudaSuccess;
+    }
+    size_t total_bytes() const {
+        size_t s = 0;
+        for (auto &kv : bufs) s += kv.second.bytes;
+        return s;
+    }
+};
+
+}  // namespace sgb
+
+struct sg_graph {
+    sg_ctx *ctx = nullptr;
+    uint32_t nv = 0;
+    uint64_t ne = 0;
+    bool weighted = false, symmetric = false, has_csc = false;
+    double weight_sum = 0.0;  // for the SSSP delta heuristic (hybrid_sssp.cu:184-197)
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
+    uint32_t *row = nullptr, *col = nullptr, *w = nullptr;
+    uint32_t *crow = nullptr, *ccol = nullptr, *cw = nullptr;
+    sgb::Workspace ws;
+};
+
+namespace sgb {
+
+inline sg_status set_error(sg_ctx *ctx, sg_status st, const char *fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return st;
+}
+
+inline sg_status cuda_status(sg_ctx *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return SG_OK;
+    set_error(ctx, e == cudaErrorMemoryAllocation ? SG_ERR_OUT_OF_MEMORY : SG_ERR_CUDA, "%s: %s", what,
+              cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? SG_ERR_OUT_OF_MEMORY : SG_ERR_CUDA;
+}
+
+#define SG_TRY_CUDA(ctx, call)                                       \
+    do {                                                             \
+        cudaError_t _e = (call);                                     \
+        if (_e != cudaSuccess) return ::sgb::cuda_status(ctx, _e, #call); \
+    } while (0)
+
+inline sg_status device_error_status(uint32_t bits) {
+    using namespace sepgraph::dev;
+    if (bits & kErrTimeout) return SG_ERR_TIMEOUT;
+    if (bits & (kErrCapacity | kErrChunkCapacity)) return SG_ERR_CAPACITY;
+    if (bits & kErrOverflow) return SG_ERR_OVERFLOW;
+    if (bits & kErrUnsupported) return SG_ERR_UNSUPPORTED;
+    return SG_OK;
+}
+
+// Is `p` device memory of the context's device (output written in place)?
+inline bool is_device_ptr(const void *p, int device) {
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == device;
+}
+
+// Engine launch description shared by the algorithm entry points.
+struct EngineConfig {
+    int scheme = 0;
+    int forced = -1;
+    int lb_push = sepgraph::engine::LB_FINE;
+    int lb_pull = sepgraph::engine::LB_FINE;
+    int priority = 0;
+    int trace = 0;
+    uint32_t max_iteration = 200;
+    double alpha = 15, beta = 18, edge_factor = 1.0;
+    unsigned long long prio_init_raw = 0, prio_step_raw = 0;
+    double timeout_s = 30.0;
+    bool blocking = true;
+    sg_round_trace *trace_out = nullptr;
+    uint32_t trace_cap = 0;
+};
+
+struct EngineResult {
+    sepgraph::engine::Ctrl ctrl{};
+    float ms = 0.f;
+};
+
+inline cudaError_t pinned(sg_ctx *ctx, size_t bytes, void **out) {
+    if (ctx->pinned_bytes < bytes) {
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        ctx->pinned = nullptr;
+        ctx->pinned_bytes = 0;
+        cudaError_t e = cudaMallocHost(&ctx->pinned, bytes);
+        if (e != cudaSuccess) return e;
+        ctx->pinned_bytes = bytes;
+    }
+    *out = ctx->pinned;
+    return cudaSuccess;
+}
+
+// Runs the engine for functor `app` on graph `g`.  `value` and `buffer` are
+// device arrays of nv elements (value may be the caller's output buffer).
+template <typename App, typename TV, typename TB, typename TW>
+sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, TB *buffer, EngineResult *res) {
+    using namespace sepgraph::engine;
+    sg_ctx *ctx = g->ctx;
+    const uint32_t nv = g->nv;
+    const uint64_t ne = g->ne;
+    KArgs<TV, TB, TW> a;
+    std::memset(&a, 0, sizeof a);
+    a.csr.nnodes = nv;
+    a.csr.nedges = (uint32_t)ne;
+    a.csr.row_start = g->row;
+    a.csr.edge_dst = g->col;
+    a.csr.edge_weights = g->w;
+    a.csc.nnodes = nv;
+    a.csc.nedges = (uint32_t)ne;
+    a.csc.col_start = g->crow;
+    a.csc.edge_source = g->ccol;
+    a.csc.edge_weights = g->cw;
+    a.csc.csr_row_start = g->row;
+    a.csr_w = g->w;
+    a.csc_w = g->cw;
+    a.value = value;
+    a.buffer = buffer;
+
+    const uint32_t nwords = (nv + 31) / 32 + 1;
+    const uint32_t heavy_threshold = 1024, chunk_edges = 1024;
+    const uint32_t heavy_cap = (uint32_t)(ne / heavy_threshold + 2);
+    const uint32_t chunk_cap = (uint32_t)(ne / chunk_edges + ne / heavy_threshold + 2);
+    auto &ws = g->ws;
+    SG_TRY_CUDA(ctx, ws.get("tmp", nv, &a.tmp));
+    SG_TRY_CUDA(ctx, ws.get("q0", nv, &a.queue[0]));
+    SG_TRY_CUDA(ctx, ws.get("q1", nv, &a.queue[1]));
+    SG_TRY_CUDA(ctx, ws.get("q2", nv, &a.queue[2]));
+    SG_TRY_CUDA(ctx, ws.get("bm0", nwords, &a.bitmap[0]));
+    SG_TRY_CUDA(ctx, ws.get("bm1", nwords, &a.bitmap[1]));
+    SG_TRY_CUDA(ctx, ws.get("fl0", nwords, &a.qflag[0]));
+    SG_TRY_CUDA(ctx, ws.get("fl1", nwords, &a.qflag[1]));
+    SG_TRY_CUDA(ctx, ws.get("middle", nv, &a.middle));
+    SG_TRY_CUDA(ctx, ws.get("heavy", heavy_cap, &a.heavy, true));
+    SG_TRY_CUDA(ctx, ws.get("chunk", chunk_cap, &a.chunk_owner, true));
+    SG_TRY_CUDA(ctx, ws.get("ctrl", 1, &a.ctrl));
+    if (cfg.trace && cfg.trace_cap) SG_TRY_CUDA(ctx, ws.get("trace", cfg.trace_cap, &a.trace));
+    a.queue_cap = nv;
+    a.nwords = nwords;
+    a.heavy_cap = heavy_cap;
+    a.chunk_cap = chunk_cap;
+    a.trace_cap = cfg.trace ? cfg.trace_cap : 0;
+
+    Params &p = a.p;
+    p.scheme = cfg.scheme;
+    p.forced = cfg.forced;
+    p.lb_push = cfg.lb_push;
+    p.lb_pull = cfg.lb_pull;
+    p.priority = cfg.priority;
+    p.trace = cfg.trace;
+    p.collect = (cfg.forced < 0 || cfg.trace) ? 1 : 0;
+    p.has_csc = g->has_csc;
+    p.max_iteration = cfg.max_iteration ? cfg.max_iteration : 200;
+    p.heavy_threshold = heavy_threshold;
+    p.chunk_edges = chunk_edges;
+    p.pull_warp_threshold = 32;
+    p.alpha = cfg.alpha;
+    p.beta = cfg.beta;
+    p.total_workload0 = (long long)((double)ne * cfg.edge_factor);
+    p.prio_init_raw = cfg.prio_init_raw;
+    p.prio_step_raw = cfg.prio_step_raw;
+    p.timeout_ns = (unsigned long long)((cfg.timeout_s > 0 ? cfg.timeout_s : 30.0) * 1e9);
+
+    // the functor sees the graph like AppBase members are set in Engine::InitGraph (framework.cuh:162-166)
+    app.m_csr_graph = a.csr;
+    app.m_csc_graph = a.csc;
+    app.m_nnodes = nv;
+    app.m_nedges = (uint32_t)ne;
+    app.m_p_current_round = &a.ctrl->round;
+
+    auto kernel = hybrid_engine_kernel<App, TV, TB, TW>;
+    static int blocks_per_sm = 0;  // one per template instantiation
+    if (blocks_per_sm == 0) {
+        SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kernel, kBlockThreads, 0));
+        if (blocks_per_sm <= 0) return set_error(ctx, SG_ERR_NO_DEVICE, "engine kernel cannot be resident");
+    }
+    dim3 grid(ctx->prop.multiProcessorCount * blocks_per_sm), block(kBlockThreads);
+
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    void *args[] = {(void *)&app, (void *)&a};
+    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)kernel, grid, block, args, 0, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    if (!cfg.blocking) return SG_OK;
+
+    void *h = nullptr;
+    SG_TRY_CUDA(ctx, pinned(ctx, sizeof(Ctrl) + sizeof(sg_round_trace) * a.trace_cap, &h));
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(h, a.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+    if (a.trace_cap)
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync((char *)h + sizeof(Ctrl), a.trace, sizeof(sg_round_trace) * a.trace_cap,
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(&res->ctrl, h, sizeof(Ctrl));
+    if (a.trace_cap && cfg.trace_out)
+        std::memcpy(cfg.trace_out, (char *)h + sizeof(Ctrl),
+                    sizeof(sg_round_trace) * std::min<uint32_t>(res->ctrl.n_trace, cfg.trace_cap));
+    SG_TRY_CUDA(ctx, cudaEventElapsedTime(&res->ms, ctx->ev0, ctx->ev1));
+    const sg_status st = device_error_status(res->ctrl.error);
+    if (st != SG_OK) return set_error(ctx, st, "device error bits 0x%x", res->ctrl.error);
+    return SG_OK;
+}
+
+inline void fill_stats(sg_stats *s, const EngineResult &r) {
+    if (!s) return;
+    s->rounds = r.ctrl.round;
+    s->max_iteration_reached = r.ctrl.max_iteration_reached;
+    for (int i = 0; i < 8; ++i) s->rounds_by_variant[i] = r.ctrl.rounds_by_variant[i];
+    s->time_kernel_ms = r.ms;
+    s->time_total_ms = r.ms;
+    s->edges_processed = r.ctrl.edges_processed;
+    s->vertices_processed = r.ctrl.vertices_processed;
+    s->device_error = r.ctrl.error;
+    s->n_trace = s->trace ? std::min<uint32_t>(r.ctrl.n_trace, s->trace_capacity) : 0;
+}
+
+}  // namespace sgb
+
+// ---------------------------------------------------------------- Engine
+// C++ mirror of the reference's Engine for custom functors.  Same lifecycle:
+// Engine(AlgoType) -> SetOptions -> LoadGraph -> InitGraph(data...) -> Start ->
+// GatherValue / GatherBuffer / PrintInfo.  LoadGraph takes the device graph
+// (the reference reads the graph named by --graphfile, framework.cuh:99-133).
+namespace sepgraph {
+namespace engine {
+
+template <typename TValue, typename TBuffer, typename TWeight,
+          template <typename, typename, typename, typename...> class TAppImpl, typename... UnusedData>
+class Engine {
+    using AppImpl = TAppImpl<TValue, TBuffer, TWeight, UnusedData...>;
+    policy::AlgoType m_algo_type;
+    common::EngineOptions m_opt;
+    sg_graph *m_graph = nullptr;
+    std::unique_ptr<AppImpl> m_app;
+    TValue *m_value = nullptr;
+    TBuffer *m_buffer = nullptr;
+    std::vector<TValue> m_value_host;
+    std::vector<TBuffer> m_buffer_host;
+    sgb::EngineResult m_res;
+    sg_status m_status = SG_OK;
+
+   public:
+    int max_iteration = 200;
+    double alpha = 15, beta = 18, edge_factor = 1.0;
+
+    explicit Engine(policy::AlgoType algo_type) : m_algo_type(algo_type) {}
+    void SetOptions(common::EngineOptions &o) { m_opt = o; }
+    void LoadGraph(sg_graph *g) { m_graph = g; }
+    void InitGraph(UnusedData &...data) { m_app.reset(new AppImpl(data...)); }
+
+    sg_status Start() {
+        if (!m_graph || !m_app) return SG_ERR_INVALID_ARG;
+        auto &ws = m_graph->ws;
+        if (ws.get("engine_value", m_graph->nv, &m_value) != cudaSuccess ||
+            ws.get("engine_buffer", m_graph->nv, &m_buffer) != cudaSuccess)
+            return SG_ERR_OUT_OF_MEMORY;
+        sgb::EngineConfig cfg;
+        cfg.scheme = m_algo_type == policy::AlgoType::TRAVERSAL_SCHEME ? 0 : 1;
+        cfg.forced = m_opt.IsForceVariant() ? m_opt.GetAlgoVariant().Id() : -1;
+        const double avg_deg = m_graph->nv ? (double)m_graph->ne / m_graph->nv : 0;
+        cfg.lb_push = m_opt.IsForceLoadBalancing(common::MsgPassing::PUSH)
+                          ? (int)m_opt.GetLoadBalancing(common::MsgPassing::PUSH)
+                          : (avg_deg >= 5 ? LB_FINE : LB_NONE);  // LoadOptions (framework.cuh:402-443)
+        cfg.lb_pull = m_opt.IsForceLoadBalancing(common::MsgPassing::PULL)
+                          ? (int)m_opt.GetLoadBalancing(common::MsgPassing::PULL)
+                          : (avg_deg >= 5 ? LB_FINE : LB_NONE);
+        cfg.priority = m_opt.GetPriorityType() == common::Priority::LOW_HIGH;
+        cfg.prio_init_raw = to_raw<TBuffer>((TBuffer)m_opt.GetPriorityThreshold());
+        cfg.prio_step_raw = cfg.prio_init_raw;
+        cfg.max_iteration = max_iteration;
+        cfg.alpha = alpha;
+        cfg.beta = beta;
+        cfg.edge_factor = edge_factor;
+        if (alpha == 0) cfg.forced = V_ASYNC_PUSH_DD;
+        m_status = sgb::run_engine<AppImpl, TValue, TBuffer, TWeight>(m_graph, *m_app, cfg, m_value, m_buffer, &m_res);
+        return m_status;
+    }
+    const std::vector<TValue> &GatherValue() {
+        m_value_host.resize(m_graph->nv);
+        cudaMemcpy(m_value_host.data(), m_value, sizeof(TValue) * m_graph->nv, cudaMemcpyDeviceToHost);
+        return m_value_host;
+    }
+    const std::vector<TBuffer> &GatherBuffer() {
+        m_buffer_host.resize(m_graph->nv);
+        cudaMemcpy(m_buffer_host.data(), m_buffer, sizeof(TBuffer) * m_graph->nv, cudaMemcpyDeviceToHost);
+        return m_buffer_host;
+    }
+    void PrintInfo() const {
+        std::printf("Kernel time: %f\nTotal rounds: %u\n", m_res.ms, m_res.ctrl.round);
+        for (int v = 0; v < 8; ++v)
+            if (m_res.ctrl.rounds_by_variant[v])
+                std::printf("  %s rounds: %u\n", common::AlgoVariant::FromId(v).ToString().c_str(),
+                            m_res.ctrl.rounds_by_variant[v]);
+    }
+    const sgb::EngineResult &Result() const { return m_res; }
+};
+
+}  // namespace engine
+}  // namespace sepgraph

@@ -1,0 +1,420 @@
+"""Python binding of libsepgraph_b200.so (the C ABI in include/sepgraph.h).
+
+Thin ctypes layer used by the tests, bench.py and scripts: host graphs are
+numpy views of the library's own buffers; device work goes through the C
+entry points only.  There is no Python or CPU fallback: if the shared
+library is missing, ``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsepgraph_b200.so")
+
+SG_OK = 0
+STATUS_NAMES = {
+    0: "SG_OK", 1: "SG_ERR_INVALID_ARG", 2: "SG_ERR_CUDA", 3: "SG_ERR_OUT_OF_MEMORY", 4: "SG_ERR_TIMEOUT",
+    5: "SG_ERR_CAPACITY", 6: "SG_ERR_UNSUPPORTED", 7: "SG_ERR_OVERFLOW", 8: "SG_ERR_NO_DEVICE", 9: "SG_ERR_IO",
+    10: "SG_ERR_FORMAT", 11: "SG_ERR_BUSY",
+}
+
+# selectors (include/sepgraph.h)
+LB = {"auto": -1, "none": 0, "coarse": 1, "fine": 2, "hybrid": 3}
+VARIANTS = {
+    "auto": -1, "sync_push_td": 0, "sync_push_dd": 1, "sync_pull_td": 2, "sync_pull_dd": 3,
+    "async_push_td": 4, "async_push_dd": 5, "async_pull_td": 6, "async_pull_dd": 7,
+}
+VARIANT_NAMES = {v: k.upper() for k, v in VARIANTS.items() if v >= 0}
+GRAPH_SYMMETRIC = 0x1
+GRAPH_NO_CSC = 0x2
+GEN_SYMMETRIC = 0x1
+GEN_KEEP_SELF_LOOPS = 0x2
+GEN_KEEP_DUPLICATES = 0x4
+INF = 0xFFFFFFFF
+
+
+class SGError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)} {detail}".strip())
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("variant", C.c_int32), ("lb_push", C.c_int32), ("lb_pull", C.c_int32), ("priority", C.c_int32),
+        ("priority_delta", C.c_double), ("cut_threshold", C.c_double), ("alpha", C.c_double),
+        ("beta", C.c_double), ("edge_factor", C.c_double), ("max_iteration", C.c_int32), ("fused", C.c_int32),
+        ("block_size", C.c_int32), ("non_atomic", C.c_int32), ("trace", C.c_int32), ("pr_error", C.c_double),
+        ("timeout_s", C.c_double), ("blocking", C.c_int32), ("reserved", C.c_int32 * 7),
+    ]
+
+
+class RoundTrace(C.Structure):
+    _fields_ = [
+        ("round", C.c_uint32), ("variant", C.c_int32), ("in_nodes", C.c_uint32), ("out_nodes", C.c_uint32),
+        ("in_workload", C.c_uint64), ("out_workload", C.c_uint64), ("total_workload", C.c_int64),
+        ("time_ms", C.c_float), ("pad", C.c_uint32),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("rounds", C.c_uint32), ("max_iteration_reached", C.c_uint32), ("rounds_by_variant", C.c_uint32 * 8),
+        ("time_total_ms", C.c_double), ("time_kernel_ms", C.c_double), ("edges_processed", C.c_uint64),
+        ("vertices_processed", C.c_uint64), ("edges_reached", C.c_uint64), ("vertices_reached", C.c_uint32),
+        ("search_depth", C.c_uint32), ("device_error", C.c_uint32), ("n_trace", C.c_uint32),
+        ("trace", C.POINTER(RoundTrace)), ("trace_capacity", C.c_uint32), ("pad", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("trace", "pad", "rounds_by_variant")}
+        d["rounds_by_variant"] = {VARIANT_NAMES[i]: int(self.rounds_by_variant[i]) for i in range(8)
+                                  if self.rounds_by_variant[i]}
+        return d
+
+
+_lib = None
+_P = C.c_void_p
+_U32P = C.POINTER(C.c_uint32)
+
+
+def load() -> C.CDLL:
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} not built (run make -C sep-graph_b200)")
+    L = C.CDLL(LIB_PATH)
+    sig = {
+        "sg_status_string": (C.c_char_p, [C.c_int]),
+        "sg_abi_version": (C.c_int, []),
+        "sg_init": (C.c_int, [C.c_int, C.POINTER(_P)]),
+        "sg_destroy": (C.c_int, [_P]),
+        "sg_ctx_set_stream": (C.c_int, [_P, _P]),
+        "sg_ctx_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
+        "sg_ctx_synchronize": (C.c_int, [_P]),
+        "sg_last_error": (C.c_char_p, [_P]),
+        "sg_device_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                     C.c_char_p, C.c_size_t]),
+        "sg_graph_create": (C.c_int, [_P, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_uint32, C.POINTER(_P)]),
+        "sg_graph_create_from_host": (C.c_int, [_P, _P, C.c_uint32, C.POINTER(_P)]),
+        "sg_graph_destroy": (C.c_int, [_P]),
+        "sg_graph_info": (C.c_int, [_P, _U32P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_int)]),
+        "sg_options_default": (C.c_int, [C.POINTER(Options)]),
+        "sg_bfs": (C.c_int, [_P, C.c_uint32, C.POINTER(Options), _P, C.POINTER(Stats)]),
+        "sg_sssp": (C.c_int, [_P, C.c_uint32, C.POINTER(Options), _P, C.POINTER(Stats)]),
+        "sg_pagerank": (C.c_int, [_P, C.POINTER(Options), _P, _P, C.POINTER(Stats)]),
+        "sg_bc": (C.c_int, [_P, C.c_uint32, C.POINTER(Options), _P, _P, C.POINTER(Stats)]),
+        "sg_hgraph_gen_rmat": (C.c_int, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                         C.c_uint64, C.c_uint32, C.POINTER(_P)]),
+        "sg_hgraph_gen_grid": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
+        "sg_hgraph_from_csr": (C.c_int, [C.c_uint32, C.c_uint64, _P, _P, _P, C.POINTER(_P)]),
+        "sg_hgraph_gen_weights": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint64]),
+        "sg_hgraph_read_gr": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
+        "sg_hgraph_write_gr": (C.c_int, [_P, C.c_char_p]),
+        "sg_hgraph_read_market": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_P)]),
+        "sg_hgraph_info": (C.c_int, [_P, _U32P, C.POINTER(C.c_uint64), C.POINTER(_U32P), C.POINTER(_U32P),
+                                     C.POINTER(_U32P)]),
+        "sg_hgraph_max_degree_vertex": (C.c_int, [_P, _U32P, _U32P]),
+        "sg_hgraph_pick_sources": (C.c_int, [_P, C.c_uint32, C.c_uint64, _U32P]),
+        "sg_hgraph_destroy": (C.c_int, [_P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(st: int, where: str, ctx=None):
+    if st != SG_OK:
+        detail = ""
+        if ctx is not None:
+            detail = load().sg_last_error(ctx).decode(errors="replace")
+        raise SGError(st, where, detail)
+
+
+def _ptr(a) -> Optional[int]:
+    """Address of a numpy array, an int device pointer, or a torch tensor."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError(type(a))
+
+
+def make_options(**kw) -> Options:
+    o = Options()
+    _check(load().sg_options_default(C.byref(o)), "sg_options_default")
+    for k, v in kw.items():
+        if v is None:
+            continue
+        if k == "variant" and isinstance(v, str):
+            v = VARIANTS[v.lower()]
+        elif k in ("lb_push", "lb_pull") and isinstance(v, str):
+            v = LB[v.lower()]
+        elif k == "priority" and isinstance(v, str):
+            v = {"none": 0, "low_high": 1, "sampling": 2}[v.lower()]
+        if not hasattr(o, k):
+            raise KeyError(f"unknown option {k}")
+        setattr(o, k, int(v) if isinstance(v, bool) else v)
+    return o
+
+
+class HostGraph:
+    """Host CSR graph owned by the library (generators and file I/O)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 1,
+             symmetric: bool = False, keep_self_loops=False, keep_duplicates=False) -> "HostGraph":
+        h = _P()
+        flags = (GEN_SYMMETRIC if symmetric else 0) | (GEN_KEEP_SELF_LOOPS if keep_self_loops else 0) | \
+            (GEN_KEEP_DUPLICATES if keep_duplicates else 0)
+        _check(load().sg_hgraph_gen_rmat(scale, edge_factor, a, b, c, seed, flags, C.byref(h)), "gen_rmat")
+        return cls(h)
+
+    @classmethod
+    def grid(cls, rows: int, cols: int) -> "HostGraph":
+        h = _P()
+        _check(load().sg_hgraph_gen_grid(rows, cols, 0, C.byref(h)), "gen_grid")
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, offsets, indices, weights=None) -> "HostGraph":
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint32)
+        if weights is not None:
+            weights = np.ascontiguousarray(weights, dtype=np.uint32)
+        h = _P()
+        _check(load().sg_hgraph_from_csr(len(offsets) - 1, len(indices), _ptr(offsets), _ptr(indices),
+                                         _ptr(weights), C.byref(h)), "from_csr")
+        return cls(h)
+
+    @classmethod
+    def read_gr(cls, path: str) -> "HostGraph":
+        h = _P()
+        _check(load().sg_hgraph_read_gr(path.encode(), C.byref(h)), "read_gr")
+        return cls(h)
+
+    @classmethod
+    def read_market(cls, path: str, symmetrize: bool = False) -> "HostGraph":
+        h = _P()
+        _check(load().sg_hgraph_read_market(path.encode(), int(symmetrize), C.byref(h)), "read_market")
+        return cls(h)
+
+    def write_gr(self, path: str):
+        _check(load().sg_hgraph_write_gr(self._h, path.encode()), "write_gr")
+
+    def gen_weights(self, lo: int, hi: int, seed: int = 2) -> "HostGraph":
+        _check(load().sg_hgraph_gen_weights(self._h, lo, hi, seed), "gen_weights")
+        return self
+
+    def _info(self):
+        nv, ne = C.c_uint32(), C.c_uint64()
+        o, i, w = _U32P(), _U32P(), _U32P()
+        _check(load().sg_hgraph_info(self._h, C.byref(nv), C.byref(ne), C.byref(o), C.byref(i), C.byref(w)),
+               "hgraph_info")
+        return nv.value, ne.value, o, i, w
+
+    @property
+    def nv(self) -> int:
+        return self._info()[0]
+
+    @property
+    def ne(self) -> int:
+        return self._info()[1]
+
+    @property
+    def offsets(self) -> np.ndarray:
+        nv, ne, o, _, _ = self._info()
+        return np.ctypeslib.as_array(o, shape=(nv + 1,))
+
+    @property
+    def indices(self) -> np.ndarray:
+        nv, ne, _, i, _ = self._info()
+        return np.ctypeslib.as_array(i, shape=(ne,)) if ne else np.zeros(0, np.uint32)
+
+    @property
+    def weights(self) -> Optional[np.ndarray]:
+        nv, ne, _, _, w = self._info()
+        if not w:
+            return None
+        return np.ctypeslib.as_array(w, shape=(ne,)) if ne else np.zeros(0, np.uint32)
+
+    def max_degree_vertex(self):
+        v, d = C.c_uint32(), C.c_uint32()
+        _check(load().sg_hgraph_max_degree_vertex(self._h, C.byref(v), C.byref(d)), "max_degree_vertex")
+        return v.value, d.value
+
+    def pick_sources(self, n: int, seed: int = 3) -> np.ndarray:
+        out = np.zeros(n, np.uint32)
+        _check(load().sg_hgraph_pick_sources(self._h, n, seed, out.ctypes.data_as(_U32P)), "pick_sources")
+        return out
+
+    def close(self):
+        if self._h:
+            load().sg_hgraph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """One CUDA device + stream (sg_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._c = _P()
+        _check(load().sg_init(device, C.byref(self._c)), "sg_init")
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._c
+
+    @property
+    def stream(self) -> int:
+        s = _P()
+        _check(load().sg_ctx_get_stream(self._c, C.byref(s)), "get_stream", self._c)
+        return s.value or 0
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        _check(load().sg_ctx_set_stream(self._c, stream_ptr), "set_stream", self._c)
+
+    def synchronize(self):
+        _check(load().sg_ctx_synchronize(self._c), "synchronize", self._c)
+
+    def device_info(self) -> dict:
+        sm, hbm, l2 = C.c_int(), C.c_uint64(), C.c_uint64()
+        name = C.create_string_buffer(256)
+        _check(load().sg_device_info(self._c, C.byref(sm), C.byref(hbm), C.byref(l2), name, 256), "device_info")
+        return {"sm_count": sm.value, "hbm_bytes": hbm.value, "l2_bytes": l2.value, "name": name.value.decode()}
+
+    def graph(self, hg: HostGraph, symmetric: bool = False, no_csc: bool = False) -> "Graph":
+        g = _P()
+        flags = (GRAPH_SYMMETRIC if symmetric else 0) | (GRAPH_NO_CSC if no_csc else 0)
+        _check(load().sg_graph_create_from_host(self._c, hg._h, flags, C.byref(g)), "graph_create", self._c)
+        return Graph(self, g)
+
+    def graph_from_csr(self, offsets, indices, weights=None, symmetric=False, no_csc=False) -> "Graph":
+        g = _P()
+        flags = (GRAPH_SYMMETRIC if symmetric else 0) | (GRAPH_NO_CSC if no_csc else 0)
+        nv = (len(offsets) - 1) if not isinstance(offsets, int) else None
+        _check(load().sg_graph_create(self._c, nv, len(indices), _ptr(offsets), _ptr(indices), _ptr(weights),
+                                      flags, C.byref(g)), "graph_create", self._c)
+        return Graph(self, g)
+
+    def close(self):
+        if self._c:
+            load().sg_destroy(self._c)
+            self._c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """Device-resident graph (sg_graph) and the four algorithms."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx = ctx
+        self._g = handle
+
+    @property
+    def handle(self):
+        return self._g
+
+    def info(self) -> dict:
+        nv, ne, b, w = C.c_uint32(), C.c_uint64(), C.c_uint64(), C.c_int()
+        _check(load().sg_graph_info(self._g, C.byref(nv), C.byref(ne), C.byref(b), C.byref(w)), "graph_info")
+        return {"nv": nv.value, "ne": ne.value, "device_bytes": b.value, "weighted": bool(w.value)}
+
+    @property
+    def nv(self) -> int:
+        return self.info()["nv"]
+
+    def _stats(self, trace_capacity: int):
+        st = Stats()
+        buf = None
+        if trace_capacity:
+            buf = (RoundTrace * trace_capacity)()
+            st.trace = C.cast(buf, C.POINTER(RoundTrace))
+            st.trace_capacity = trace_capacity
+        return st, buf
+
+    @staticmethod
+    def _trace(buf, st):
+        if buf is None:
+            return None
+        return [{k: getattr(buf[i], k) for k, _ in RoundTrace._fields_ if k != "pad"} for i in range(st.n_trace)]
+
+    def _prep(self, out, dtype, trace_capacity, opts):
+        o = make_options(**opts)
+        if trace_capacity:
+            o.trace = 1
+        if out is None:
+            out = np.empty(self.nv, dtype)
+        st, buf = self._stats(trace_capacity)
+        return o, out, st, buf
+
+    def bfs(self, source: int, out=None, trace_capacity: int = 0, **opts):
+        o, out, st, buf = self._prep(out, np.uint32, trace_capacity, opts)
+        _check(load().sg_bfs(self._g, source, C.byref(o), _ptr(out), C.byref(st)), "sg_bfs", self.ctx.handle)
+        return out, st, self._trace(buf, st)
+
+    def sssp(self, source: int, out=None, trace_capacity: int = 0, **opts):
+        o, out, st, buf = self._prep(out, np.uint32, trace_capacity, opts)
+        _check(load().sg_sssp(self._g, source, C.byref(o), _ptr(out), C.byref(st)), "sg_sssp", self.ctx.handle)
+        return out, st, self._trace(buf, st)
+
+    def pagerank(self, out=None, residual_out=None, trace_capacity: int = 0, **opts):
+        o, out, st, buf = self._prep(out, np.float32, trace_capacity, opts)
+        _check(load().sg_pagerank(self._g, C.byref(o), _ptr(out), _ptr(residual_out), C.byref(st)), "sg_pagerank",
+               self.ctx.handle)
+        return out, st, self._trace(buf, st)
+
+    def bc(self, source: int, out=None, sigma_out=None, trace_capacity: int = 0, **opts):
+        o = make_options(**opts)
+        if trace_capacity:
+            o.trace = 1
+        if out is None:
+            out = np.empty(self.nv, np.float32)
+        if sigma_out is None:
+            sigma_out = np.empty(self.nv, np.uint64)
+        st, buf = self._stats(trace_capacity)
+        _check(load().sg_bc(self._g, source, C.byref(o), _ptr(out), _ptr(sigma_out), C.byref(st)), "sg_bc",
+               self.ctx.handle)
+        return out, sigma_out, st
+
+    def close(self):
+        if self._g:
+            load().sg_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

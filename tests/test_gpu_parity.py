@@ -1,0 +1,212 @@
+"""GPU parity of the four algorithms through the C ABI against the oracle.
+
+Tolerances (stated per algorithm, as the reference's checkers are):
+  BFS levels, SSSP distances (uint32 weights): bit-exact.
+  PageRank: L1 distance of L1-normalised rank vectors <= 1e-6 against the
+            FP64 restatement of PageRankHost run to a 1e-12 residual.
+  BC: |gpu - fp64| <= 1e-4 * |fp64| + 1e-5 per vertex; path counts exact.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import sepgraph as sg
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GIDS = [os.path.basename(p)[:-4] for p in GOLDEN]
+PR_L1_TOL = 1e-6
+BC_RTOL, BC_ATOL = 1e-4, 1e-5
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = sg.Context(0)
+    yield c
+    c.close()
+
+
+def _load(path):
+    z = np.load(path)
+    return {k: z[k] for k in z.files}
+
+
+def _graph(ctx, g, weighted=True, symmetric=False):
+    return ctx.graph_from_csr(g["offsets"], g["indices"], g["weights"] if weighted and len(g["indices"]) else None,
+                              symmetric=symmetric)
+
+
+TRAVERSAL_VARIANTS = ["auto", "async_push_dd", "async_pull_dd"]
+LBS = ["none", "fine"]
+
+
+@pytest.mark.parametrize("lb", LBS)
+@pytest.mark.parametrize("variant", TRAVERSAL_VARIANTS)
+@pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
+def test_bfs_golden(ctx, path, variant, lb):
+    g = _load(path)
+    G = _graph(ctx, g, weighted=False)
+    for non_atomic in (1, 0):
+        lv, st, _ = G.bfs(int(g["source"]), variant=variant, lb_push=lb, lb_pull=lb, non_atomic=non_atomic)
+        assert (lv == g["bfs"]).all(), (variant, lb, non_atomic)
+
+
+@pytest.mark.parametrize("lb", LBS)
+@pytest.mark.parametrize("variant", TRAVERSAL_VARIANTS + ["async_push_td", "prio"])
+@pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
+def test_sssp_golden(ctx, path, variant, lb):
+    g = _load(path)
+    G = _graph(ctx, g)
+    kw = dict(lb_push=lb, lb_pull=lb, max_iteration=100000)
+    if variant == "prio":
+        kw.update(priority="low_high")
+    else:
+        kw.update(variant=variant)
+    d, st, _ = G.sssp(int(g["source"]), **kw)
+    assert (d == g["sssp"]).all(), (variant, lb)
+
+
+def _pr_l1(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a / a.sum() - b / b.sum()).sum()
+
+
+@pytest.mark.parametrize("variant", ["auto", "sync_pull_td", "async_push_td", "async_push_dd"])
+@pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
+def test_pagerank_golden(ctx, path, variant):
+    g = _load(path)
+    G = _graph(ctx, g, weighted=False)
+    r, st, _ = G.pagerank(variant=variant, pr_error=1e-7, max_iteration=100000)
+    ref64 = oracle.pagerank_f64(g["offsets"], g["indices"], 1e-12)
+    assert _pr_l1(r, ref64) <= PR_L1_TOL, (variant, _pr_l1(r, ref64))
+    # the reference's own 5% checker at its default threshold
+    r2, _, _ = G.pagerank(variant=variant, pr_error=float(g["pr0_error"]), max_iteration=100000)
+    if oracle.ref_available():
+        assert oracle.ref_pagerank_check(r2, g["pr0"]) == 0
+
+
+@pytest.mark.parametrize("variant", TRAVERSAL_VARIANTS)
+@pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
+def test_bc_golden(ctx, path, variant):
+    g = _load(path)
+    G = _graph(ctx, g, weighted=False)
+    src = int(g["source"])
+    bc, sigma, st = G.bc(src, variant=variant)
+    bc64, sig64, _ = oracle.bc_f64(g["offsets"], g["indices"], src)
+    assert (sigma.astype(np.float64) == sig64).all()
+    assert np.allclose(bc, bc64, rtol=BC_RTOL, atol=BC_ATOL), np.max(np.abs(bc - bc64))
+    assert np.allclose(bc, g["bc"], rtol=0.05, atol=0.01)  # reference float result, its 5% rule
+
+
+# ---------------------------------------------------------------- larger graphs, oracle at test time
+@pytest.mark.parametrize("scale,sym", [(14, True), (16, True), (15, False)])
+def test_bfs_rmat(ctx, scale, sym):
+    h = sg.HostGraph.rmat(scale, 16, symmetric=sym, seed=1)
+    G = ctx.graph(h, symmetric=sym)
+    for src in [h.max_degree_vertex()[0]] + list(h.pick_sources(3, 3)):
+        ref = oracle.bfs(h.offsets, h.indices, int(src))
+        for variant in ("auto", "async_push_dd", "async_pull_dd"):
+            lv, st, _ = G.bfs(int(src), variant=variant)
+            assert (lv == ref).all(), (variant, src)
+        assert st.edges_reached == np.diff(h.offsets)[ref != sg.INF].sum()
+
+
+@pytest.mark.parametrize("scale", [14, 16])
+def test_sssp_rmat(ctx, scale):
+    h = sg.HostGraph.rmat(scale, 16, symmetric=False, seed=1).gen_weights(1, 64, 2)
+    G = ctx.graph(h)
+    for src in h.pick_sources(4, 3):
+        ref = oracle.sssp(h.offsets, h.indices, h.weights, int(src))
+        for kw in (dict(), dict(variant="async_push_dd"), dict(priority="low_high"),
+                   dict(priority="low_high", priority_delta=8), dict(variant="async_pull_dd")):
+            d, st, _ = G.sssp(int(src), max_iteration=100000, **kw)
+            assert (d == ref).all(), kw
+
+
+def test_sssp_grid(ctx):
+    h = sg.HostGraph.grid(128, 96).gen_weights(1, 1000, 2)
+    G = ctx.graph(h)
+    ref = oracle.sssp(h.offsets, h.indices, h.weights, 0)
+    for kw in (dict(), dict(priority="low_high"), dict(variant="async_push_dd", lb_push="none")):
+        d, st, _ = G.sssp(0, max_iteration=1000000, **kw)
+        assert (d == ref).all(), kw
+
+
+@pytest.mark.parametrize("variant", ["auto", "sync_pull_td", "async_push_dd"])
+def test_pagerank_rmat(ctx, variant):
+    h = sg.HostGraph.rmat(14, 16, symmetric=False, seed=1)
+    G = ctx.graph(h)
+    r, st, _ = G.pagerank(variant=variant, pr_error=1e-7, max_iteration=100000)
+    ref64 = oracle.pagerank_f64(h.offsets, h.indices, 1e-12)
+    assert _pr_l1(r, ref64) <= PR_L1_TOL
+
+
+def test_bc_rmat(ctx):
+    h = sg.HostGraph.rmat(14, 16, symmetric=True, seed=1)
+    G = ctx.graph(h, symmetric=True)
+    for src in [h.max_degree_vertex()[0], int(h.pick_sources(1, 3)[0])]:
+        bc, sigma, st = G.bc(int(src))
+        bc64, sig64, _ = oracle.bc_f64(h.offsets, h.indices, int(src))
+        assert (sigma.astype(np.float64) == sig64).all()
+        assert np.allclose(bc, bc64, rtol=BC_RTOL, atol=BC_ATOL)
+
+
+# ---------------------------------------------------------------- engine behaviour
+def test_policy_switches_direction_and_trace(ctx):
+    h = sg.HostGraph.rmat(16, 16, symmetric=True, seed=1)
+    G = ctx.graph(h, symmetric=True)
+    src = h.max_degree_vertex()[0]
+    lv, st, tr = G.bfs(src, trace_capacity=64)
+    assert st.rounds_by_variant[7] > 0 and st.rounds_by_variant[5] > 0, "push and pull rounds"
+    assert len(tr) == st.rounds and tr[0]["variant"] == 5
+    assert tr[-1]["out_nodes"] == 0
+    assert (lv == oracle.bfs(h.offsets, h.indices, src)).all()
+
+
+def test_forced_unsupported_variant(ctx):
+    g = _load(GOLDEN[0])
+    G = _graph(ctx, g)
+    for v in ("async_pull_td", "sync_push_td", "sync_push_dd"):
+        with pytest.raises(sg.SGError) as e:
+            G.bfs(0, variant=v)
+        assert e.value.status == 6
+    G.bfs(0)  # context still usable
+
+
+def test_invalid_source(ctx):
+    g = _load(GOLDEN[0])
+    G = _graph(ctx, g)
+    with pytest.raises(sg.SGError) as e:
+        G.bfs(len(g["offsets"]) - 1)
+    assert e.value.status == 1
+
+
+def test_max_iteration_stops(ctx):
+    g = _load([p for p in GOLDEN if "chain16" in p][0])
+    G = _graph(ctx, g)
+    lv, st, _ = G.bfs(0, max_iteration=5, variant="async_push_dd")
+    assert st.rounds == 5 and st.max_iteration_reached == 1
+    assert (lv[:5] == np.arange(5)).all() and (lv[6:] == sg.INF).all()
+
+
+def test_device_output_buffer(ctx):
+    torch = pytest.importorskip("torch")
+    h = sg.HostGraph.rmat(12, 16, symmetric=True, seed=1)
+    G = ctx.graph(h, symmetric=True)
+    out = torch.empty(h.nv, dtype=torch.int32, device="cuda")
+    G.bfs(0, out=out)
+    ctx.synchronize()
+    ref = oracle.bfs(h.offsets, h.indices, 0)
+    assert (out.cpu().numpy().view(np.uint32) == ref).all()
+
+
+def test_repeat_runs_deterministic(ctx):
+    h = sg.HostGraph.rmat(13, 16, symmetric=False, seed=3).gen_weights(1, 64, 2)
+    G = ctx.graph(h)
+    outs = [G.sssp(int(h.pick_sources(1, 1)[0]))[0] for _ in range(3)]
+    assert all((o == outs[0]).all() for o in outs)

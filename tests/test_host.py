@@ -1,0 +1,174 @@
+"""Host-side logic of the library (no GPU): seeded generators, CSR build,
+graph file formats, source selection, and the C ABI symbol table."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import sepgraph as sg
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _rows_sorted_unique(off, idx):
+    for v in range(len(off) - 1):
+        r = idx[off[v]:off[v + 1]]
+        if len(r) > 1 and not (np.diff(r.astype(np.int64)) > 0).all():
+            return False
+    return True
+
+
+def test_rmat_properties_symmetric():
+    h = sg.HostGraph.rmat(12, 16, symmetric=True, seed=1)
+    off, idx = h.offsets, h.indices
+    assert h.nv == 4096 and off[0] == 0 and off[-1] == h.ne == len(idx)
+    src = np.repeat(np.arange(h.nv, dtype=np.uint32), np.diff(off))
+    assert not (src == idx).any(), "self-loops removed"
+    assert _rows_sorted_unique(off, idx), "rows sorted, duplicates removed"
+    fwd = set(zip(src.tolist(), idx.tolist()))
+    assert all((d, s) in fwd for s, d in list(fwd)[:5000]), "symmetric"
+    assert h.ne <= 2 * 16 * 4096
+
+
+def test_rmat_deterministic_and_seeded():
+    a = sg.HostGraph.rmat(11, 8, seed=3)
+    b = sg.HostGraph.rmat(11, 8, seed=3)
+    c = sg.HostGraph.rmat(11, 8, seed=4)
+    assert (a.offsets == b.offsets).all() and (a.indices == b.indices).all()
+    assert a.ne != c.ne or not (a.indices == c.indices).all()
+
+
+def test_rmat_skew_matches_quadrant_probabilities():
+    # a+b = 0.76 of edges leave the lower half of the id space at every level
+    h = sg.HostGraph.rmat(14, 16, symmetric=False, seed=1, keep_duplicates=True, keep_self_loops=True)
+    src = np.repeat(np.arange(h.nv), np.diff(h.offsets))
+    frac_low = (src < h.nv // 2).mean()
+    assert abs(frac_low - 0.76) < 0.01
+    dst = h.indices
+    assert abs((dst < h.nv // 2).mean() - 0.76) < 0.01
+    assert h.ne == 16 * h.nv
+
+
+def test_grid_structure():
+    h = sg.HostGraph.grid(5, 7)
+    assert h.nv == 35 and h.ne == 2 * (5 * 6 + 4 * 7)
+    off, idx = h.offsets, h.indices
+    assert _rows_sorted_unique(off, idx)
+    # corner (0,0) has right and down neighbours
+    assert list(idx[off[0]:off[1]]) == [1, 7]
+    # interior vertex (2,3) -> 17 has 4 neighbours
+    assert list(idx[off[17]:off[18]]) == [10, 16, 18, 24]
+
+
+def test_weights_range_and_seed():
+    h = sg.HostGraph.rmat(10, 16, seed=1).gen_weights(1, 64, 2)
+    w = h.weights
+    assert w.min() >= 1 and w.max() < 64 and len(w) == h.ne
+    h2 = sg.HostGraph.rmat(10, 16, seed=1).gen_weights(1, 64, 2)
+    assert (h2.weights == w).all()
+    assert abs(w.mean() - 32) < 1.0
+
+
+def test_max_degree_vertex_lowest_id_on_ties():
+    off = np.array([0, 2, 4, 5], np.uint32)
+    idx = np.array([1, 2, 0, 2, 0], np.uint32)
+    h = sg.HostGraph.from_csr(off, idx)
+    assert h.max_degree_vertex() == (0, 2)
+
+
+def test_pick_sources_have_out_edges():
+    h = sg.HostGraph.rmat(12, 16, seed=1)
+    s = h.pick_sources(8, 3)
+    deg = np.diff(h.offsets)
+    assert len(set(s.tolist())) == 8 and (deg[s] > 0).all()
+    assert (h.pick_sources(8, 3) == s).all()
+
+
+def test_gr_roundtrip(tmp_path):
+    h = sg.HostGraph.rmat(9, 16, seed=2).gen_weights(1, 100, 5)
+    p = str(tmp_path / "g.gr")
+    h.write_gr(p)
+    g = sg.HostGraph.read_gr(p)
+    assert (g.offsets == h.offsets).all() and (g.indices == h.indices).all() and (g.weights == h.weights).all()
+    # unweighted, odd edge count
+    u = sg.HostGraph.from_csr(np.array([0, 1, 3, 3], np.uint32), np.array([1, 0, 2], np.uint32))
+    u.write_gr(p)
+    g = sg.HostGraph.read_gr(p)
+    assert g.weights is None and list(g.indices) == [1, 0, 2]
+
+
+def test_gr_layout_matches_galois_v1(tmp_path):
+    """Header {1, 4, nv, ne}, u64 row ends, u32 dsts, pad on odd ne, u32 weights (parser.cpp:409-506)."""
+    u = sg.HostGraph.from_csr(np.array([0, 2, 3], np.uint32), np.array([1, 0, 0], np.uint32),
+                              np.array([5, 6, 7], np.uint32))
+    p = str(tmp_path / "g.gr")
+    u.write_gr(p)
+    raw = open(p, "rb").read()
+    hdr = np.frombuffer(raw[:32], np.uint64)
+    assert list(hdr) == [1, 4, 2, 3]
+    assert list(np.frombuffer(raw[32:48], np.uint64)) == [2, 3]
+    assert list(np.frombuffer(raw[48:60], np.uint32)) == [1, 0, 0]
+    assert list(np.frombuffer(raw[64:76], np.uint32)) == [5, 6, 7]
+    assert len(raw) == 76
+
+
+def test_gr_rejects_malformed(tmp_path):
+    p = tmp_path / "bad.gr"
+    p.write_bytes(np.array([2, 0, 3, 1], np.uint64).tobytes())
+    with pytest.raises(sg.SGError) as e:
+        sg.HostGraph.read_gr(str(p))
+    assert e.value.status == 10
+    with pytest.raises(sg.SGError) as e:
+        sg.HostGraph.read_gr(str(tmp_path / "missing.gr"))
+    assert e.value.status == 9
+
+
+def test_market_reader_dedups_sorted(tmp_path):
+    p = tmp_path / "m.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate integer general\n% c\n4 4 6\n1 2 3\n1 2 3\n2 1 4\n4 3 1\n1 3 2\n3 3 9\n")
+    g = sg.HostGraph.read_market(str(p))
+    assert list(g.offsets) == [0, 2, 3, 4, 5]
+    assert list(g.indices) == [1, 2, 0, 2, 2]
+    assert list(g.weights) == [3, 2, 4, 9, 1]
+
+
+def test_from_csr_validates():
+    with pytest.raises(sg.SGError):
+        sg.HostGraph.from_csr(np.array([0, 2, 1], np.uint32), np.array([0, 1], np.uint32))
+    with pytest.raises(sg.SGError):
+        sg.HostGraph.from_csr(np.array([0, 1], np.uint32), np.array([5], np.uint32))
+
+
+def test_abi_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "sepgraph.h")).read()
+    declared = set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(sg_\w+)\s*\(", hdr, re.M))
+    assert len(declared) > 20
+    out = subprocess.run(["nm", "-D", "--defined-only", sg.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (sg_\w+)", out))
+    missing = declared - exported
+    assert not missing, missing
+    lib = sg.load()
+    for name in declared:
+        assert hasattr(lib, name)
+
+
+def test_no_device_reports_status_not_crash():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(sg.SGError) as e:
+        sg.Context(0)
+    assert e.value.status == 8
+
+
+def test_options_defaults_match_reference_flags():
+    o = sg.make_options()
+    assert o.alpha == 15 and o.beta == 18 and o.max_iteration == 200  # app_skeleton.h:44-51
+    assert o.non_atomic == 1  # hybrid_bfs main.cpp:37
+    assert abs(o.pr_error - 0.01) < 1e-12  # hybrid_pr main.cpp:37
+    assert o.variant == -1 and o.lb_push == -1 and o.blocking == 1
