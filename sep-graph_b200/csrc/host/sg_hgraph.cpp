@@ -221,6 +221,34 @@ sg_status gen_grid(uint32_t rows, uint32_t cols, uint32_t flags, HostGraph &g) {
     return SG_OK;
 }
 
+sg_status gen_random(uint32_t nv, uint32_t gen_factor, uint64_t seed, HostGraph &g) {
+    if (nv < 2 || gen_factor < 1 || gen_factor >= nv) return SG_ERR_INVALID_ARG;
+    g.nv = nv;
+    g.offsets.assign(nv + 1, 0);
+    std::vector<uint32_t> deg(nv);
+    const uint64_t stream = splitmix64(seed ^ 0x6E6E6E6EULL);
+    for (uint32_t v = 0; v < nv; ++v) deg[v] = 1 + (uint32_t)(splitmix64(stream + 2ull * v) % gen_factor);
+    for (uint32_t v = 0; v < nv; ++v) g.offsets[v + 1] = g.offsets[v] + deg[v];
+    g.ne = g.offsets[nv];
+    g.indices.resize(g.ne);
+    parallel_for(nv, [&](uint64_t b, uint64_t e) {
+        for (uint64_t v = b; v < e; ++v) {
+            uint64_t st = splitmix64(stream + 2ull * v + 1);
+            uint32_t *row = g.indices.data() + g.offsets[v];
+            uint32_t n = 0;
+            while (n < deg[v]) {
+                st = splitmix64(st);
+                const uint32_t u = (uint32_t)(st % nv);
+                if (u == v || std::find(row, row + n, u) != row + n) continue;
+                row[n++] = u;
+            }
+            std::sort(row, row + n);
+        }
+    });
+    g.weights.clear();
+    return SG_OK;
+}
+
 sg_status gen_weights(HostGraph &g, uint32_t lo, uint32_t hi, uint64_t seed) {
     if (hi <= lo) return SG_ERR_INVALID_ARG;
     const uint64_t span = hi - lo;

@@ -21,6 +21,7 @@ unsigned host_threads();
 sg_status gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed, uint32_t flags,
                    HostGraph &g);
 sg_status gen_grid(uint32_t rows, uint32_t cols, uint32_t flags, HostGraph &g);
+sg_status gen_random(uint32_t nv, uint32_t gen_factor, uint64_t seed, HostGraph &g);
 sg_status gen_weights(HostGraph &g, uint32_t lo, uint32_t hi, uint64_t seed);
 sg_status from_csr(uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices, const uint32_t *weights,
                    HostGraph &g);

@@ -1,0 +1,98 @@
+// hybrid_bc: flags and flow of samples/hybrid_bc (main.cpp, hybrid_bc.cu:303-412).
+// --check compares path counts exactly and BC values with the sample's 5%
+// rule (hybrid_bc_host.cpp:94-127) against a double-precision Brandes pass.
+#include <algorithm>
+#include <cmath>
+
+#include "sg_skeleton.h"
+
+DEFINE_int32(source_node, 0, "The source node for the BFS traversal (clamped to [0, nnodes-1])");
+DEFINE_bool(sparse, false, "use async/push/dd + fusion for high-diameter");
+DEFINE_int32(src, 0, "The source node of BC algorithm");
+
+static void HostBC(const LoadedGraph &g, uint32_t s, std::vector<double> &bc, std::vector<double> &sigma) {
+    std::vector<int64_t> lv(g.nv, -1);
+    bc.assign(g.nv, 0.0);
+    sigma.assign(g.nv, 0.0);
+    std::vector<uint32_t> order;
+    lv[s] = 0;
+    sigma[s] = 1;
+    std::deque<uint32_t> q{s};
+    while (!q.empty()) {
+        uint32_t u = q.front();
+        q.pop_front();
+        order.push_back(u);
+        for (uint32_t e = g.off[u]; e < g.off[u + 1]; ++e) {
+            uint32_t w = g.idx[e];
+            if (lv[w] < 0) {
+                lv[w] = lv[u] + 1;
+                q.push_back(w);
+            }
+            if (lv[w] == lv[u] + 1) sigma[w] += sigma[u];
+        }
+    }
+    for (size_t i = order.size(); i-- > 0;) {
+        uint32_t u = order[i];
+        if (u == s) continue;
+        for (uint32_t e = g.off[u]; e < g.off[u + 1]; ++e) {
+            uint32_t w = g.idx[e];
+            if (lv[w] == lv[u] + 1) bc[u] += sigma[u] / sigma[w] * (1.0 + bc[w]);
+        }
+    }
+    for (auto &x : bc) x *= 0.5;
+}
+
+static bool HybridBC() {
+    LoadedGraph g;
+    if (!LoadGraph(g)) return false;
+    const uint32_t src = (uint32_t)std::min<int64_t>(std::max<int64_t>(0, FLAGS_source_node), g.nv - 1);
+    sg_options o = CommonOptions();
+    if (FLAGS_sparse) {
+        o.fused = 1;
+        o.variant = SG_ASYNC_PUSH_DD;
+        o.lb_push = SG_LB_NONE;
+    } else {
+        o.lb_push = SG_LB_FINE_GRAINED;
+        o.lb_pull = SG_LB_FINE_GRAINED;
+    }
+    std::vector<float> bc(g.nv);
+    std::vector<uint64_t> sigma(g.nv);
+    std::vector<sg_round_trace> trace(FLAGS_trace ? std::max(1, FLAGS_max_iteration) : 0);
+    sg_stats st{};
+    st.trace = trace.empty() ? nullptr : trace.data();
+    st.trace_capacity = (uint32_t)trace.size();
+    JsonRecord js;
+    SG_CHECK(sg_bc(g.dev, src, &o, bc.data(), sigma.data(), &st));
+    PrintRun(st, o, js);
+    bool ok = true;
+    if (FLAGS_check) {
+        std::vector<double> rb, rs;
+        HostBC(g, src, rb, rs);
+        for (uint32_t v = 0; v < std::min<uint32_t>(10, g.nv); ++v) std::printf("%u %f %f\n", v, rb[v], bc[v]);
+        int es = 0, eb = 0;
+        for (uint32_t v = 0; v < g.nv; ++v) {
+            es += (double)sigma[v] != rs[v];
+            const double err = std::fabs(bc[v]) < 0.01 ? std::fabs(bc[v] - rb[v]) : std::fabs((bc[v] - rb[v]) / rb[v]);
+            eb += err > 0.05;
+        }
+        std::printf("Checking sigmas...\nTotal errors: %d\nChecking BC values...\nTotal errors: %d\n", es, eb);
+        ok = es == 0 && eb == 0;
+    } else {
+        std::printf("Warning: Result not checked\n");
+    }
+    if (!FLAGS_output.empty()) {
+        FILE *f = std::fopen(FLAGS_output.c_str(), "w");
+        for (uint32_t v = 0; f && v < g.nv; ++v) std::fprintf(f, "%u %f\n", v, bc[v]);
+        if (f) std::fclose(f);
+    }
+    sg_graph_destroy(g.dev);
+    return ok;
+}
+
+struct App {
+    static const char *Name() { return "bc"; }
+    static const char *NameUpper() { return "BC"; }
+    static bool Single() { return HybridBC(); }
+};
+
+int main(int argc, char **argv) { return Skeleton<App>()(argc, argv); }

@@ -199,6 +199,7 @@ sgb::EngineConfig make_config(const sg_graph *g, const sg_options &o, int scheme
     c.edge_factor = o.edge_factor;
     if (o.alpha == 0) c.forced = engine::V_ASYNC_PUSH_DD;  // framework.cuh:445-448
     c.timeout_s = o.timeout_s;
+    c.blocks_per_sm = o.blocks_per_sm;
     c.blocking = o.blocking != 0;
     if (o.trace && stats && stats->trace && stats->trace_capacity) {
         c.trace = 1;
@@ -301,6 +302,8 @@ sg_status sg_init(int device, sg_ctx **out) {
 
 sg_status sg_destroy(sg_ctx *ctx) {
     if (!ctx) return SG_ERR_INVALID_ARG;
+    if (ctx->live_graphs > 0)
+        return set_error(ctx, SG_ERR_BUSY, "%d graph(s) of this context still exist", ctx->live_graphs);
     DeviceGuard dg(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -451,6 +454,7 @@ sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t 
         delete g;
         return st;
     }
+    ctx->live_graphs++;
     *out = g;
     return SG_OK;
 }
@@ -466,6 +470,7 @@ sg_status sg_graph_destroy(sg_graph *g) {
     DeviceGuard dg(g->ctx->device);
     cudaStreamSynchronize(g->ctx->stream);
     if (g->arena) cudaFree(g->arena);
+    g->ctx->live_graphs--;
     delete g;
     return SG_OK;
 }
@@ -691,6 +696,19 @@ sg_status sg_hgraph_gen_grid(uint32_t rows, uint32_t cols, uint32_t flags, sg_hg
     sg_hgraph *h = new (std::nothrow) sg_hgraph;
     if (!h) return SG_ERR_OUT_OF_MEMORY;
     sg_status st = sgb::gen_grid(rows, cols, flags, *h);
+    if (st != SG_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return SG_OK;
+}
+
+sg_status sg_hgraph_gen_random(uint32_t nv, uint32_t gen_factor, uint64_t seed, sg_hgraph **out) {
+    if (!out) return SG_ERR_INVALID_ARG;
+    sg_hgraph *h = new (std::nothrow) sg_hgraph;
+    if (!h) return SG_ERR_OUT_OF_MEMORY;
+    sg_status st = sgb::gen_random(nv, gen_factor, seed, *h);
     if (st != SG_OK) {
         delete h;
         return st;

@@ -19,14 +19,18 @@
 //   ASYNC_PUSH_TD  all-vertex push (async_push_td.cuh:25-147).
 // TD rounds end with RebuildArrayWorklist (algo_variants.cuh:58-76).
 //
-// Frontier bookkeeping lives on the device: every append to the next worklist
-// also accumulates the appended vertex's out-degree (the "scout count" that
-// SumOutDegreeQueue computes with a separate kernel and a D2H copy,
-// driver.cuh:225-248), so the policy needs no extra pass.  The last block to
-// reach each grid barrier evaluates the policy, rotates worklists and records
-// the trace.  A per-vertex "queued" bitmap keeps each worklist free of
-// duplicates, which bounds every worklist by |V| (the reference sizes them at
-// 0.2*|E| and can overflow silently, graph_datum.cuh:90).
+// Control: block 0 is the fixed leader.  At every grid barrier it waits for
+// the other blocks, evaluates the policy from the round's atomic counters
+// (every append to the next worklist also accumulates the appended vertex's
+// out-degree — the "scout count" that SumOutDegreeQueue computes with a separate
+// kernel and a D2H copy, driver.cuh:225-248), rotates worklists, records the
+// trace and publishes a 64-byte round snapshot that every block reads with
+// four vector loads.  Policy state (RunningInfo, hybrid_policy.h:36-120) stays
+// in the leader thread's local memory for the whole launch.
+//
+// A per-vertex "queued" bitmap keeps each worklist free of duplicates, which
+// bounds every worklist by |V| (the reference sizes them at 0.2*|E| and can
+// overflow silently, graph_datum.cuh:90).
 #pragma once
 #include <cstdint>
 #include <cstring>
@@ -57,6 +61,7 @@ enum : int32_t {
 __host__ __device__ inline bool is_dd(int v) { return v & 1; }
 __host__ __device__ inline bool is_pull(int v) { return (v >> 1) & 1; }
 __host__ __device__ inline bool is_sync(int v) { return ((v >> 2) & 1) == 0; }
+__host__ __device__ inline bool is_pull_dd(int v) { return v >= 0 && is_dd(v) && is_pull(v); }
 
 enum : int32_t { LB_NONE = 0, LB_COARSE = 1, LB_FINE = 2, LB_HYBRID = 3 };
 
@@ -66,29 +71,35 @@ struct HeavyItem {
     TBuffer payload;
 };
 
-// Engine control block (device memory).  Field roles mirror RunningInfo
-// (hybrid_policy.h:36-120) plus the worklist slot assignment.
-struct Ctrl {
-    uint32_t bar_count, bar_gen, error, done;
-    uint32_t round, max_iteration_reached;
+// Round snapshot: written by the leader, read by every block after a barrier.
+struct alignas(16) RoundState {
     int32_t variant, last_variant;
-    uint32_t qin, qhi, qlo, bin, bout, dirty, pile, in_flag;
-    uint32_t qcount[3];
-    uint32_t heavy_enq[3];
-    unsigned long long scout[3];
-    uint32_t middle_count, heavy_count, chunk_count, inspect_next;
-    long long total_workload;
-    uint32_t input_active, output_active;
-    unsigned long long input_workload, output_workload;
+    uint32_t round, done;
+    uint32_t qin, qhi, qlo, bin;
+    uint32_t bout, dirty, pile, F;
+    uint32_t heavy_expected, pad;
     unsigned long long prio_raw;
-    float policy_time[8];
-    uint32_t policy_seen;
-    float time_per_work;
-    unsigned long long t_round_start, t_start, t_end;
+};
+static_assert(sizeof(RoundState) == 64, "snapshot is four 16-byte loads");
+
+// Updated atomically by all blocks during a round.
+struct Counters {
+    uint32_t qcount[4];
+    uint32_t heavy_enq[4];
+    unsigned long long scout[4];
+    uint32_t middle_count, heavy_count, chunk_count, error;
+    unsigned long long edges_processed;
+};
+
+struct Ctrl {
+    uint32_t bar_count, bar_gen, pad0, pad1;
+    RoundState rs;
+    Counters cnt;
+    // results, written by the leader when the loop ends
+    uint32_t round, max_iteration_reached, n_trace, error;
     uint32_t rounds_by_variant[8];
     unsigned long long edges_processed, vertices_processed;
-    uint32_t n_trace;
-    uint32_t pad;
+    unsigned long long t_start, t_end;
 };
 
 struct Params {
@@ -134,11 +145,19 @@ struct KArgs {
     Params p;
 };
 
-// Round snapshot broadcast through shared memory after every barrier.
-struct Snap {
-    int32_t variant, last_variant;
-    uint32_t round, qin, qhi, qlo, bin, bout, dirty, pile, in_flag, F, heavy_expected, done;
-    unsigned long long prio_raw;
+// Leader-only policy state (RunningInfo), lives in block 0 / thread 0.
+struct PolicyState {
+    RoundState rs;
+    long long total_workload;
+    uint32_t input_active, output_active;
+    unsigned long long input_workload, output_workload;
+    float policy_time[8];
+    uint32_t policy_seen, inspect_next;
+    float time_per_work;
+    unsigned long long t_round_start, t_start;
+    uint32_t rounds_by_variant[8];
+    unsigned long long vertices_processed;
+    uint32_t n_trace, max_iteration_reached;
 };
 
 template <typename TBuffer>
@@ -209,9 +228,63 @@ __device__ __forceinline__ int accumulate(App &app, const uint32_t *w, uint32_t 
 __device__ __forceinline__ bool acc_success(int st) { return st < 2; }
 __device__ __forceinline__ bool acc_continue(int st) { return st & 1; }
 
+// Bounded grid barrier with block 0 as the fixed leader.  Every other block
+// publishes its writes (fence) and arrives; block 0 waits for all arrivals,
+// runs `leader()` on one thread, and releases the generation.  A wait that
+// exceeds timeout_ns raises kErrTimeout (the leader still releases, so every
+// block leaves the kernel at its next status check) and returns false.
+template <typename Leader>
+__device__ __forceinline__ bool grid_sync(Ctrl *c, unsigned long long timeout_ns, Leader &&leader) {
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t ok = 1;
+        const uint32_t g = dev::ld_acquire(&c->bar_gen);
+        if (blockIdx.x == 0) {
+            const uint32_t need = gridDim.x - 1;
+            const uint64_t t0 = dev::globaltimer_ns();
+            uint32_t spins = 0;
+            while (dev::ld_acquire(&c->bar_count) < need) {
+                ++spins;
+                if ((spins & 255u) == 0 && (dev::globaltimer_ns() - t0 > timeout_ns || spins > (1u << 28))) {
+                    atomicOr(&c->cnt.error, dev::kErrTimeout);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+            __threadfence();
+            c->bar_count = 0;
+            if (ok) leader();
+            __threadfence();
+            dev::st_release(&c->bar_gen, g + 1);
+        } else {
+            __threadfence();
+            atomicAdd(&c->bar_count, 1u);
+            const uint64_t t0 = dev::globaltimer_ns();
+            uint32_t spins = 0;
+            while (dev::ld_acquire(&c->bar_gen) == g) {
+                ++spins;
+                if ((spins & 255u) == 0 && (dev::globaltimer_ns() - t0 > timeout_ns || spins > (1u << 28))) {
+                    atomicOr(&c->cnt.error, dev::kErrTimeout);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __threadfence();
+        if (dev::ld_l2(&c->cnt.error) & dev::kErrTimeout) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 template <typename App, typename TV, typename TB, typename TW>
 struct EngineKernel {
     using Args = KArgs<TV, TB, TW>;
+    using Snap = RoundState;
 
     static __device__ __forceinline__ uint32_t gthread() { return blockIdx.x * blockDim.x + threadIdx.x; }
     static __device__ __forceinline__ uint32_t nthreads() { return gridDim.x * blockDim.x; }
@@ -227,11 +300,12 @@ struct EngineKernel {
         uint32_t h0 = dev::warp_sum(acc.heavy_hi), h1 = dev::warp_sum(acc.heavy_lo);
         unsigned long long ed = dev::warp_sum(acc.edges);
         if (dev::lane_id() == 0) {
-            if (s0) atomicAdd(&a.ctrl->scout[q_hi], s0);
-            if (h0) atomicAdd(&a.ctrl->heavy_enq[q_hi], h0);
-            if (s1) atomicAdd(&a.ctrl->scout[q_lo], s1);
-            if (h1) atomicAdd(&a.ctrl->heavy_enq[q_lo], h1);
-            if (ed) atomicAdd(&a.ctrl->edges_processed, ed);
+            Counters *n = &a.ctrl->cnt;
+            if (s0) atomicAdd(&n->scout[q_hi], s0);
+            if (h0) atomicAdd(&n->heavy_enq[q_hi], h0);
+            if (s1) atomicAdd(&n->scout[q_lo], s1);
+            if (h1) atomicAdd(&n->heavy_enq[q_lo], h1);
+            if (ed) atomicAdd(&n->edges_processed, ed);
         }
         acc.reset();
     }
@@ -241,41 +315,43 @@ struct EngineKernel {
     // its out-degree for the policy.  All 32 lanes must call.
     static __device__ __forceinline__ void enqueue(App &app, const Args &a, const Snap &s, uint32_t dst, bool want,
                                                    Acc &acc) {
+        Counters *n = &a.ctrl->cnt;
         bool hi = true;
         if (a.p.priority && want) hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), dev::ld_l2(a.buffer + dst));
         bool w_hi = want && hi, w_lo = want && !hi;
         if (want) __threadfence();  // order the buffer update before publishing the queued bit
         if (w_hi) w_hi = dev::bitmap_set(a.qflag[0], dst);
         if (w_lo) w_lo = dev::bitmap_set(a.qflag[1], dst);
-        dev::warp_append(a.queue[s.qhi], &a.ctrl->qcount[s.qhi], a.queue_cap, w_hi, dst, &a.ctrl->error);
-        if (a.p.priority) dev::warp_append(a.queue[s.qlo], &a.ctrl->qcount[s.qlo], a.queue_cap, w_lo, dst,
-                                           &a.ctrl->error);
+        dev::warp_append(a.queue[s.qhi], &n->qcount[s.qhi], a.queue_cap, w_hi, dst, &n->error);
+        if (a.p.priority) dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, w_lo, dst, &n->error);
         if (w_hi || w_lo) acc.count(w_hi, out_degree(a, dst), a.p.heavy_threshold);
     }
 
     // Single-thread enqueue (LB NONE paths run divergent per-thread loops).
     static __device__ __forceinline__ void enqueue_one(App &app, const Args &a, const Snap &s, uint32_t dst,
                                                        Acc &acc) {
+        Counters *n = &a.ctrl->cnt;
         bool hi = true;
         if (a.p.priority) hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), dev::ld_l2(a.buffer + dst));
         __threadfence();
         const int k = hi ? 0 : 1;
         if (!dev::bitmap_set(a.qflag[k], dst)) return;
         const uint32_t q = hi ? s.qhi : s.qlo;
-        const uint32_t pos = atomicAdd(&a.ctrl->qcount[q], 1u);
+        const uint32_t pos = atomicAdd(&n->qcount[q], 1u);
         if (pos < a.queue_cap)
             a.queue[q][pos] = dst;
         else
-            atomicOr(&a.ctrl->error, dev::kErrCapacity);
+            atomicOr(&n->error, dev::kErrCapacity);
         acc.count(hi, out_degree(a, dst), a.p.heavy_threshold);
     }
 
     static __device__ __forceinline__ void register_heavy(const Args &a, uint32_t src, uint32_t beg, uint32_t deg,
                                                           TB payload) {
+        Counters *n = &a.ctrl->cnt;
         const uint32_t ce = a.p.chunk_edges;
         const uint32_t nch = (deg + ce - 1) / ce;
-        const uint32_t idx = atomicAdd(&a.ctrl->heavy_count, 1u);
-        const uint32_t cb = atomicAdd(&a.ctrl->chunk_count, nch);
+        const uint32_t idx = atomicAdd(&n->heavy_count, 1u);
+        const uint32_t cb = atomicAdd(&n->chunk_count, nch);
         if (idx < a.heavy_cap && cb <= a.chunk_cap && nch <= a.chunk_cap - cb) {
             HeavyItem<TB> h;
             h.src = src;
@@ -286,14 +362,23 @@ struct EngineKernel {
             a.heavy[idx] = h;
             for (uint32_t i = 0; i < nch; ++i) a.chunk_owner[cb + i] = idx;
         } else {
-            atomicOr(&a.ctrl->error, dev::kErrChunkCapacity);
+            atomicOr(&n->error, dev::kErrChunkCapacity);
         }
     }
 
+    // Owner lane of edge e in a warp's concatenated edge lists: the largest k
+    // with excl[k] <= e (binary search over the exclusive degree scan).
+    static __device__ __forceinline__ uint32_t owner(const uint32_t *excl, uint32_t e) {
+        uint32_t k = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1)
+            if (excl[k + step] <= e) k += step;
+        return k;
+    }
+
     // Warp-cooperative expansion of up to 32 (src, beg, deg, payload) items:
-    // the warp walks the concatenation of their edge lists 32 edges at a time,
-    // each lane locating its source by binary search over the warp's exclusive
-    // degree scan (shared memory).  All 32 lanes must call.
+    // the warp walks the concatenation of their edge lists 32 edges at a time.
+    // All 32 lanes must call.
     static __device__ void expand_warp(App &app, const Args &a, const Snap &s, WarpLB<TB> &w, uint32_t src,
                                        uint32_t beg, uint32_t deg, TB payload, bool dd, Acc &acc) {
         const uint32_t lane = dev::lane_id();
@@ -310,10 +395,7 @@ struct EngineKernel {
             bool want = false;
             uint32_t dst = 0;
             if (e < total) {
-                uint32_t k = 0;
-#pragma unroll
-                for (uint32_t step = 16; step > 0; step >>= 1)
-                    if (w.excl[k + step] <= e) k += step;
+                const uint32_t k = owner(w.excl, e);
                 const uint32_t edge = w.beg[k] + (e - w.excl[k]);
                 dst = a.csr.edge_dest(edge);
                 const int st = accumulate<App, TB, TW>(app, a.csr_w, w.src[k], dst, edge, a.buffer + dst, w.pay[k]);
@@ -344,8 +426,8 @@ struct EngineKernel {
 
     // Chunks of heavy vertices registered in phase A, spread over all warps.
     static __device__ void heavy_phase(App &app, const Args &a, const Snap &s, bool dd, Acc &acc) {
-        const uint32_t C = min(dev::ld_l2(&a.ctrl->chunk_count), a.chunk_cap);
-        const uint32_t H = min(dev::ld_l2(&a.ctrl->heavy_count), a.heavy_cap);
+        const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count), a.chunk_cap);
+        const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count), a.heavy_cap);
         const uint32_t lane = dev::lane_id();
         const uint32_t ce = a.p.chunk_edges;
         for (uint32_t ch = gwarp(); ch < C; ch += nwarps()) {
@@ -398,6 +480,7 @@ struct EngineKernel {
         const uint32_t N = dd ? s.F : a.csr.nnodes;
         const uint32_t *Q = a.queue[s.qin];
         const TB prio = from_raw<TB>(s.prio_raw);
+        Counters *n = &a.ctrl->cnt;
         for (uint32_t base = gwarp() * 32; base < N; base += nwarps() * 32) {
             const uint32_t i = base + lane;
             const bool valid = i < N;
@@ -408,7 +491,7 @@ struct EngineKernel {
                 v = dd ? dev::ld_l2(Q + i) : i;
                 if (dd) {
                     if (s.pile) {
-                        // far pile: vertices still below the priority window stay in the pile
+                        // far pile: vertices still outside the priority window stay in the pile
                         if (!app.App::IsHighPriority(prio, dev::ld_l2(a.buffer + v))) {
                             keep = true;
                             proceed = false;
@@ -422,8 +505,7 @@ struct EngineKernel {
             }
             if (dd) {
                 __threadfence();  // pop (queued bit cleared) before reading the vertex state
-                if (s.pile) dev::warp_append(a.queue[s.qlo], &a.ctrl->qcount[s.qlo], a.queue_cap, keep, v,
-                                             &a.ctrl->error);
+                if (s.pile) dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, keep, v, &n->error);
                 if (keep) acc.count(false, out_degree(a, v), a.p.heavy_threshold);
             }
             TB payload{};
@@ -457,6 +539,7 @@ struct EngineKernel {
     static __device__ void combine_all(App &app, const Args &a, bool sync) {
         const uint32_t lane = dev::lane_id();
         const uint32_t N = a.csr.nnodes;
+        Counters *n = &a.ctrl->cnt;
         for (uint32_t base = gwarp() * 32; base < N; base += nwarps() * 32) {
             const uint32_t v = base + lane;
             bool want = false;
@@ -468,7 +551,7 @@ struct EngineKernel {
                     a.buffer[v] = pr.first;
                 want = pr.second;
             }
-            dev::warp_append(a.middle, &a.ctrl->middle_count, a.csr.nnodes, want, v, &a.ctrl->error);
+            dev::warp_append(a.middle, &n->middle_count, a.csr.nnodes, want, v, &n->error);
         }
     }
 
@@ -478,15 +561,6 @@ struct EngineKernel {
         const TB *srcbuf = sync ? a.tmp : a.buffer;
         const uint32_t *bin = a.bitmap[s.bin];
         bool hit = false;
-        if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value) {
-            if (!dd) {
-                TB r = app.PullIdentity();
-                for (uint32_t e = beg; e < beg + deg; ++e) r = app.PullReduce(r, dev::ld_l2(srcbuf + a.csc.edge_src(e)));
-                acc.edges += deg;
-                if (deg) hit = acc_success(accumulate<App, TB, TW>(app, a.csc_w, v, v, beg, a.buffer + v, r));
-                return hit;
-            }
-        }
         uint32_t e = beg;
         for (; e < beg + deg; ++e) {
             const uint32_t u = a.csc.edge_src(e);
@@ -508,20 +582,6 @@ struct EngineKernel {
         const uint32_t lane = dev::lane_id();
         const TB *srcbuf = sync ? a.tmp : a.buffer;
         const uint32_t *bin = a.bitmap[s.bin];
-        if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value) {
-            if (!dd) {
-                TB r = app.PullIdentity();
-                for (uint32_t k = lane; k < deg; k += 32) r = app.PullReduce(r, dev::ld_l2(srcbuf + a.csc.edge_src(beg + k)));
-#pragma unroll
-                for (int d = 16; d > 0; d >>= 1) r = app.PullReduce(r, __shfl_xor_sync(dev::kFullMask, r, d));
-                bool hit = false;
-                if (lane == 0) {
-                    hit = acc_success(accumulate<App, TB, TW>(app, a.csc_w, v, v, beg, a.buffer + v, r));
-                    acc.edges += deg;
-                }
-                return __shfl_sync(dev::kFullMask, hit, 0);
-            }
-        }
         bool hit = false;
         uint32_t scanned = 0;
         for (uint32_t off = 0; off < deg; off += 32) {
@@ -546,8 +606,9 @@ struct EngineKernel {
     static __device__ void pull_phase(App &app, const Args &a, const Snap &s, bool dd, bool sync, int lb,
                                       Acc &acc) {
         const uint32_t lane = dev::lane_id();
-        const uint32_t M = min(dev::ld_l2(&a.ctrl->middle_count), a.csr.nnodes);
+        const uint32_t M = min(dev::ld_l2(&a.ctrl->cnt.middle_count), a.csr.nnodes);
         const bool natural = (M == a.csr.nnodes);  // every vertex scheduled: keep CSC order
+        Counters *n = &a.ctrl->cnt;
         for (uint32_t base = gwarp() * 32; base < M; base += nwarps() * 32) {
             const uint32_t i = base + lane;
             const bool valid = i < M;
@@ -577,8 +638,89 @@ struct EngineKernel {
                     dev::bitmap_set(a.bitmap[s.bout], v);
                     want = dev::bitmap_set(a.qflag[0], v);
                 }
-                dev::warp_append(a.queue[s.qhi], &a.ctrl->qcount[s.qhi], a.queue_cap, want, v, &a.ctrl->error);
+                dev::warp_append(a.queue[s.qhi], &n->qcount[s.qhi], a.queue_cap, want, v, &n->error);
                 if (want) acc.count(true, out_degree(a, v), a.p.heavy_threshold);
+            }
+        }
+    }
+
+    // Topology-driven pull for functors with PullReduce: the warp walks the
+    // concatenated in-edge lists of 32 destinations (edge-balanced), folds the
+    // pulled values per destination in shared memory and issues one
+    // AccumulateBuffer per destination.  Destinations above heavy_threshold
+    // in-edges are split into chunks handled by pull_reduce_chunks.
+    static __device__ void pull_reduce_td(App &app, const Args &a, const Snap &s, WarpLB<TB> &w, Acc &acc) {
+        if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value) {
+            const uint32_t lane = dev::lane_id();
+            const uint32_t N = a.csr.nnodes;
+            const TB *srcbuf = a.tmp;
+            for (uint32_t base = gwarp() * 32; base < N; base += nwarps() * 32) {
+                const uint32_t v = base + lane;
+                uint32_t beg = 0, deg = 0;
+                if (v < N) {
+                    beg = a.csc.begin_edge(v);
+                    deg = a.csc.end_edge(v) - beg;
+                }
+                if (deg > a.p.heavy_threshold) {
+                    register_heavy(a, v, beg, deg, app.PullIdentity());
+                    deg = 0;
+                }
+                const uint32_t incl = dev::warp_inclusive_scan(deg);
+                const uint32_t total = __shfl_sync(dev::kFullMask, incl, 31);
+                w.excl[lane] = incl - deg;
+                w.beg[lane] = beg;
+                w.pay[lane] = app.PullIdentity();
+                __syncwarp();
+                for (uint32_t eb = 0; eb < total; eb += 32) {
+                    const uint32_t e = eb + lane;
+                    uint32_t k = 0xffffffffu;
+                    TB x = app.PullIdentity();
+                    if (e < total) {
+                        k = owner(w.excl, e);
+                        x = dev::ld_l2(srcbuf + a.csc.edge_src(w.beg[k] + (e - w.excl[k])));
+                    }
+                    // segmented reduction: lanes of one destination are contiguous
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const TB y = __shfl_down_sync(dev::kFullMask, x, d);
+                        const uint32_t ky = __shfl_down_sync(dev::kFullMask, k, d);
+                        if (lane + d < 32 && ky == k) x = app.PullReduce(x, y);
+                    }
+                    const uint32_t kp = __shfl_up_sync(dev::kFullMask, k, 1);
+                    if (e < total && (lane == 0 || kp != k)) w.pay[k] = app.PullReduce(w.pay[k], x);
+                    __syncwarp();
+                }
+                __syncwarp();
+                if (v < N && deg > 0) accumulate<App, TB, TW>(app, a.csc_w, v, v, beg, a.buffer + v, w.pay[lane]);
+                if (lane == 0) acc.edges += total;
+                __syncwarp();
+            }
+        }
+    }
+
+    static __device__ void pull_reduce_chunks(App &app, const Args &a, Acc &acc) {
+        if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value) {
+            const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count), a.chunk_cap);
+            const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count), a.heavy_cap);
+            const uint32_t lane = dev::lane_id();
+            const uint32_t ce = a.p.chunk_edges;
+            for (uint32_t ch = gwarp(); ch < C; ch += nwarps()) {
+                const uint32_t e = dev::ld_l2(a.chunk_owner + ch);
+                if (e >= H) continue;
+                const HeavyItem<TB> h = a.heavy[e];
+                if (ch < h.chunk_base) continue;
+                const uint32_t off = (ch - h.chunk_base) * ce;
+                if (off >= h.deg) continue;
+                const uint32_t len = min(ce, h.deg - off);
+                TB r = app.PullIdentity();
+                for (uint32_t k = lane; k < len; k += 32)
+                    r = app.PullReduce(r, dev::ld_l2(a.tmp + a.csc.edge_src(h.beg + off + k)));
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) r = app.PullReduce(r, __shfl_xor_sync(dev::kFullMask, r, d));
+                if (lane == 0) {
+                    accumulate<App, TB, TW>(app, a.csc_w, h.src, h.src, h.beg, a.buffer + h.src, r);
+                    acc.edges += len;
+                }
             }
         }
     }
@@ -587,86 +729,104 @@ struct EngineKernel {
     static __device__ void rebuild(App &app, const Args &a, uint32_t slot, Acc &acc) {
         const uint32_t lane = dev::lane_id();
         const uint32_t N = a.csr.nnodes;
+        Counters *n = &a.ctrl->cnt;
         for (uint32_t base = gwarp() * 32; base < N; base += nwarps() * 32) {
             const uint32_t v = base + lane;
             bool act = false;
             if (v < N) act = app.App::IsActiveNode(v, dev::ld_l2(a.buffer + v));
             if (act) act = dev::bitmap_set(a.qflag[0], v);
-            dev::warp_append(a.queue[slot], &a.ctrl->qcount[slot], a.queue_cap, act, v, &a.ctrl->error);
+            dev::warp_append(a.queue[slot], &n->qcount[slot], a.queue_cap, act, v, &n->error);
             if (act) acc.count(true, out_degree(a, v), a.p.heavy_threshold);
         }
     }
 
-    // ---------------------------------------------------------------- leader work
-    static __device__ void pre_bookkeeping(const Args &a, Ctrl *c, int var) {
-        if (!a.p.collect) return;
-        if (is_dd(var)) {
-            c->input_active = c->qcount[c->qin];
-            c->input_workload = is_pull(var) ? 0ull : c->scout[c->qin];
-            c->total_workload -= (long long)c->input_workload;
-            if (c->total_workload < 0) c->total_workload = 0;
-        } else {
-            c->input_workload = a.csr.nedges;
-            c->input_active = a.csr.nnodes;
-        }
-    }
-
-    static __device__ void reset_slot(Ctrl *c, uint32_t q) {
-        c->qcount[q] = 0;
-        c->scout[q] = 0;
-        c->heavy_enq[q] = 0;
-    }
-
+    // ---------------------------------------------------------------- leader (block 0, thread 0)
     static __device__ bool supported(const Args &a, int v) {
         if (v == V_SYNC_PUSH_TD || v == V_SYNC_PUSH_DD || v == V_ASYNC_PULL_TD) return false;
         if (is_pull(v) && !a.p.has_csc) return false;
         return true;
     }
 
-    static __device__ void leader_start(App &app, const Args &a) {
-        Ctrl *c = a.ctrl;
-        c->round = 1;
-        c->last_variant = -1;
-        int v = a.p.forced >= 0 ? a.p.forced : (a.p.scheme == 0 ? V_ASYNC_PUSH_DD : V_SYNC_PULL_TD);
-        c->inspect_next = 1;
-        c->variant = v;
-        c->qin = 0;
-        c->qhi = 1;
-        c->qlo = 2;
-        c->bin = 0;
-        c->bout = 1;
-        c->dirty = 0;
-        c->pile = 0;
-        c->in_flag = 0;
-        c->total_workload = a.p.total_workload0;
-        c->prio_raw = a.p.prio_init_raw;
-        pre_bookkeeping(a, c, v);
-        if (!supported(a, v)) {
-            c->error |= dev::kErrUnsupported;
-            c->done = 1;
+    // PreComputation's statistics for the round about to run (framework.cuh:528-568).
+    static __device__ void pre_bookkeeping(const Args &a, PolicyState &ps, uint32_t qin_count,
+                                           unsigned long long qin_scout) {
+        const int var = ps.rs.variant;
+        if (!a.p.collect) return;
+        if (is_dd(var)) {
+            ps.input_active = qin_count;
+            ps.input_workload = is_pull(var) ? 0ull : qin_scout;
+            ps.total_workload -= (long long)ps.input_workload;
+            if (ps.total_workload < 0) ps.total_workload = 0;
+        } else {
+            ps.input_workload = a.csr.nedges;
+            ps.input_active = a.csr.nnodes;
         }
-        c->t_start = c->t_round_start = dev::globaltimer_ns();
     }
 
-    static __device__ int traversal_policy(const Args &a, const Ctrl *c, int var) {
+    static __device__ void publish(const Args &a, const PolicyState &ps) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(&ps.rs);
+        uint4 *dst = reinterpret_cast<uint4 *>(&a.ctrl->rs);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) __stcg(dst + k, src[k]);
+    }
+
+    static __device__ void finish(const Args &a, PolicyState &ps, unsigned long long now) {
+        Ctrl *c = a.ctrl;
+        ps.rs.done = 1;
+        c->round = ps.rs.round;
+        c->max_iteration_reached = ps.max_iteration_reached;
+        c->n_trace = ps.n_trace;
+        for (int k = 0; k < 8; ++k) c->rounds_by_variant[k] = ps.rounds_by_variant[k];
+        c->vertices_processed = ps.vertices_processed;
+        c->t_start = ps.t_start;
+        c->t_end = now;
+    }
+
+    static __device__ void leader_start(const Args &a, PolicyState &ps) {
+        Counters *n = &a.ctrl->cnt;
+        memset(&ps, 0, sizeof ps);
+        RoundState &rs = ps.rs;
+        rs.round = 1;
+        rs.last_variant = -1;
+        rs.variant = a.p.forced >= 0 ? a.p.forced : (a.p.scheme == 0 ? V_ASYNC_PUSH_DD : V_SYNC_PULL_TD);
+        ps.inspect_next = 1;
+        rs.qin = 0;
+        rs.qhi = 1;
+        rs.qlo = 2;
+        rs.bin = 0;
+        rs.bout = 1;
+        rs.F = min(dev::ld_l2(&n->qcount[0]), a.queue_cap);
+        rs.heavy_expected = dev::ld_l2(&n->heavy_enq[0]);
+        rs.prio_raw = a.p.prio_init_raw;
+        ps.total_workload = a.p.total_workload0;
+        pre_bookkeeping(a, ps, rs.F, dev::ld_l2(&n->scout[0]));
+        ps.t_start = ps.t_round_start = dev::globaltimer_ns();
+        if (!supported(a, rs.variant)) {
+            atomicOr(&n->error, dev::kErrUnsupported);
+            finish(a, ps, ps.t_start);
+        }
+        publish(a, ps);
+    }
+
+    static __device__ int traversal_policy(const Args &a, const PolicyState &ps, int var) {
         // GetNextPolicy, TRAVERSAL_SCHEME (hybrid_policy.h:265-288)
-        if (is_pull(var) && (double)c->output_active > (double)a.csr.nnodes / a.p.beta) return V_ASYNC_PULL_DD;
-        if ((double)c->output_workload > (double)c->total_workload / a.p.alpha) return V_ASYNC_PULL_DD;
+        if (is_pull(var) && (double)ps.output_active > (double)a.csr.nnodes / a.p.beta) return V_ASYNC_PULL_DD;
+        if ((double)ps.output_workload > (double)ps.total_workload / a.p.alpha) return V_ASYNC_PULL_DD;
         return V_ASYNC_PUSH_DD;
     }
 
-    static __device__ int iterative_policy(const Args &a, Ctrl *c, int var) {
+    static __device__ int iterative_policy(PolicyState &ps, int var) {
         // Inspect SYNC_PULL_TD, ASYNC_PUSH_TD, ASYNC_PUSH_DD once each (std::set order,
         // hybrid_policy.h:180-195), then pick the smallest predicted time (130-169, 242-263).
         const int order[3] = {V_SYNC_PULL_TD, V_ASYNC_PUSH_TD, V_ASYNC_PUSH_DD};
-        if (c->inspect_next < 3) return order[c->inspect_next++];
-        if (is_dd(var) && c->input_workload > 0) c->time_per_work = c->policy_time[var] / (float)c->input_workload;
+        if (ps.inspect_next < 3) return order[ps.inspect_next++];
+        if (is_dd(var) && ps.input_workload > 0) ps.time_per_work = ps.policy_time[var] / (float)ps.input_workload;
         int best = -1;
         float bt = 0.f;
         for (int k = 0; k < 3; ++k) {
             const int v = order[k];
-            if (!(c->policy_seen & (1u << v))) continue;
-            const float t = is_dd(v) ? c->time_per_work * (float)c->output_workload : c->policy_time[v];
+            if (!(ps.policy_seen & (1u << v))) continue;
+            const float t = is_dd(v) ? ps.time_per_work * (float)ps.output_workload : ps.policy_time[v];
             if (best < 0 || t < bt) {
                 best = v;
                 bt = t;
@@ -675,110 +835,111 @@ struct EngineKernel {
         return best < 0 ? var : best;
     }
 
-    static __device__ void leader_end_round(App &app, const Args &a) {
-        Ctrl *c = a.ctrl;
-        const int var = c->variant;
-        app.App::PostComputation();
-        c->rounds_by_variant[var & 7]++;
-        const unsigned long long now = dev::globaltimer_ns();
-        const float round_ms = (float)(now - c->t_round_start) * 1e-6f;
-        c->vertices_processed += is_dd(var) ? c->qcount[c->qin] : a.csr.nnodes;
-        const bool prio_push = a.p.priority && var == V_ASYNC_PUSH_DD;
-        const uint32_t out_hi = c->qcount[c->qhi];
-        const uint32_t out_lo = prio_push ? c->qcount[c->qlo] : 0;
-        c->output_active = out_hi + out_lo;
-        if (a.p.collect) {
-            if (!is_dd(var) || !is_pull(var))
-                c->output_workload = c->scout[c->qhi] + (prio_push ? c->scout[c->qlo] : 0ull);
-            else
-                c->output_workload = 1;  // framework.cuh:790
+    static __device__ void leader_end_round(App &app, const Args &a, PolicyState &ps) {
+        Counters *n = &a.ctrl->cnt;
+        RoundState &rs = ps.rs;
+        const int var = rs.variant;
+        // counters of this round (independent loads)
+        uint32_t qc[3], he[3];
+        unsigned long long sc[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            qc[k] = dev::ld_l2(&n->qcount[k]);
+            he[k] = dev::ld_l2(&n->heavy_enq[k]);
+            sc[k] = dev::ld_l2(&n->scout[k]);
         }
-        c->policy_time[var & 7] = round_ms;
-        c->policy_seen |= 1u << (var & 7);
-        if (a.p.trace && a.trace && c->n_trace < a.trace_cap) {
+        const uint32_t err = dev::ld_l2(&n->error);
+        app.App::PostComputation();
+        ps.rounds_by_variant[var & 7]++;
+        const unsigned long long now = dev::globaltimer_ns();
+        const float round_ms = (float)(now - ps.t_round_start) * 1e-6f;
+        ps.vertices_processed += is_dd(var) ? rs.F : a.csr.nnodes;
+        const bool prio_push = a.p.priority && var == V_ASYNC_PUSH_DD;
+        const uint32_t out_hi = qc[rs.qhi];
+        const uint32_t out_lo = prio_push ? qc[rs.qlo] : 0;
+        ps.output_active = out_hi + out_lo;
+        if (a.p.collect) {
+            if (!is_pull_dd(var))
+                ps.output_workload = sc[rs.qhi] + (prio_push ? sc[rs.qlo] : 0ull);
+            else
+                ps.output_workload = 1;  // framework.cuh:790
+        }
+        ps.policy_time[var & 7] = round_ms;
+        ps.policy_seen |= 1u << (var & 7);
+        if (a.p.trace && a.trace && ps.n_trace < a.trace_cap) {
             sg_round_trace t;
-            t.round = c->round;
+            t.round = rs.round;
             t.variant = var;
-            t.in_nodes = c->input_active;
-            t.out_nodes = c->output_active;
-            t.in_workload = c->input_workload;
-            t.out_workload = c->output_workload;
-            t.total_workload = c->total_workload;
+            t.in_nodes = ps.input_active;
+            t.out_nodes = ps.output_active;
+            t.in_workload = ps.input_workload;
+            t.out_workload = ps.output_workload;
+            t.total_workload = ps.total_workload;
             t.time_ms = round_ms;
             t.pad = 0;
-            a.trace[c->n_trace] = t;
-            c->n_trace++;
+            a.trace[ps.n_trace++] = t;
         }
         int next = var;
-        if (a.p.forced < 0) next = a.p.scheme == 0 ? traversal_policy(a, c, var) : iterative_policy(a, c, var);
-        const bool fatal = (c->error & (dev::kErrTimeout | dev::kErrCapacity | dev::kErrChunkCapacity |
-                                        dev::kErrUnsupported | dev::kErrOverflow)) != 0;
-        if (c->output_active == 0 || c->round >= a.p.max_iteration || fatal) {
-            c->max_iteration_reached = c->output_active != 0 && c->round >= a.p.max_iteration;
-            c->done = 1;
-            c->t_end = now;
+        if (a.p.forced < 0) next = a.p.scheme == 0 ? traversal_policy(a, ps, var) : iterative_policy(ps, var);
+        const bool fatal = (err & (dev::kErrTimeout | dev::kErrCapacity | dev::kErrChunkCapacity |
+                                   dev::kErrUnsupported | dev::kErrOverflow)) != 0;
+        if (ps.output_active == 0 || rs.round >= a.p.max_iteration || fatal) {
+            ps.max_iteration_reached = ps.output_active != 0 && rs.round >= a.p.max_iteration;
+            finish(a, ps, now);
+            publish(a, ps);
             return;
         }
         // rotate worklists
+        uint32_t reset_q;
         if (prio_push && out_hi == 0) {
             // near pile drained: open the next priority window over the far pile (driver.cuh:668-675)
-            c->prio_raw = to_raw<TB>((TB)(from_raw<TB>(c->prio_raw) + from_raw<TB>(a.p.prio_step_raw)));
-            const uint32_t t = c->qin;
-            c->qin = c->qlo;
-            c->qlo = t;
-            reset_slot(c, c->qlo);
-            c->pile = 1;
-            c->in_flag = 1;
+            rs.prio_raw = to_raw<TB>((TB)(from_raw<TB>(rs.prio_raw) + from_raw<TB>(a.p.prio_step_raw)));
+            const uint32_t t = rs.qin;
+            rs.qin = rs.qlo;
+            rs.qlo = t;
+            reset_q = rs.qlo;
+            rs.pile = 1;
         } else {
-            const uint32_t t = c->qin;
-            c->qin = c->qhi;
-            c->qhi = t;
-            reset_slot(c, c->qhi);
-            c->pile = 0;
-            c->in_flag = 0;
+            const uint32_t t = rs.qin;
+            rs.qin = rs.qhi;
+            rs.qhi = t;
+            reset_q = rs.qhi;
+            rs.pile = 0;
         }
-        if (is_dd(var) && is_pull(var)) {
-            const uint32_t t = c->bin;
-            c->bin = c->bout;
-            c->bout = t;
-            c->dirty = (is_dd(next) && is_pull(next)) ? (1u << c->bout) : 3u;
+        n->qcount[reset_q] = 0;
+        n->scout[reset_q] = 0;
+        n->heavy_enq[reset_q] = 0;
+        if (is_pull_dd(var)) {
+            const uint32_t t = rs.bin;
+            rs.bin = rs.bout;
+            rs.bout = t;
+            rs.dirty = is_pull_dd(next) ? (1u << rs.bout) : 3u;
         } else {
-            c->dirty = 0;
+            rs.dirty = 0;
         }
         if (!supported(a, next)) {
-            c->error |= dev::kErrUnsupported;
-            c->done = 1;
-            c->t_end = now;
+            atomicOr(&n->error, dev::kErrUnsupported);
+            finish(a, ps, now);
+            publish(a, ps);
             return;
         }
-        c->last_variant = var;
-        c->variant = next;
-        c->round++;
-        c->middle_count = 0;
-        c->heavy_count = 0;
-        c->chunk_count = 0;
-        pre_bookkeeping(a, c, next);
-        c->t_round_start = dev::globaltimer_ns();
+        rs.last_variant = var;
+        rs.variant = next;
+        rs.round++;
+        rs.F = min(qc[rs.qin], a.queue_cap);
+        rs.heavy_expected = he[rs.qin];
+        n->middle_count = 0;
+        n->heavy_count = 0;
+        n->chunk_count = 0;
+        pre_bookkeeping(a, ps, rs.F, sc[rs.qin]);
+        publish(a, ps);
+        ps.t_round_start = dev::globaltimer_ns();
     }
 
     static __device__ void load_snap(const Args &a, Snap &s) {
-        if (threadIdx.x == 0) {
-            const Ctrl *c = a.ctrl;
-            s.variant = dev::ld_l2(&c->variant);
-            s.last_variant = dev::ld_l2(&c->last_variant);
-            s.round = dev::ld_l2(&c->round);
-            s.qin = dev::ld_l2(&c->qin);
-            s.qhi = dev::ld_l2(&c->qhi);
-            s.qlo = dev::ld_l2(&c->qlo);
-            s.bin = dev::ld_l2(&c->bin);
-            s.bout = dev::ld_l2(&c->bout);
-            s.dirty = dev::ld_l2(&c->dirty);
-            s.pile = dev::ld_l2(&c->pile);
-            s.in_flag = dev::ld_l2(&c->in_flag);
-            s.F = min(dev::ld_l2(&c->qcount[s.qin]), a.queue_cap);
-            s.heavy_expected = dev::ld_l2(&c->heavy_enq[s.qin]);
-            s.done = dev::ld_l2(&c->done);
-            s.prio_raw = dev::ld_l2(&c->prio_raw);
+        if (threadIdx.x < 4) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(&a.ctrl->rs);
+            reinterpret_cast<uint4 *>(&s)[threadIdx.x] = __ldcg(src + threadIdx.x);
         }
         __syncthreads();
     }
@@ -793,13 +954,14 @@ struct EngineKernel {
 template <typename App, typename TV, typename TB, typename TW>
 __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App app_in, KArgs<TV, TB, TW> a) {
     using K = EngineKernel<App, TV, TB, TW>;
-    __shared__ Snap s;
+    __shared__ RoundState s;
     __shared__ WarpLB<TB> wlb[kWarpsPerBlock];
     App app = app_in;
     Ctrl *c = a.ctrl;
-    const uint64_t tmo = a.p.timeout_ns;
+    const unsigned long long tmo = a.p.timeout_ns;
     Acc acc;
     acc.reset();
+    PolicyState ps;  // meaningful in block 0 / thread 0 only
     auto nop = [] {};
 
     // InitGraph (driver.cuh:68-92) and all frontier state cleared.
@@ -815,25 +977,25 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
         a.qflag[0][w] = 0;
         a.qflag[1][w] = 0;
     }
-    if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, nop)) return;
+    if (!grid_sync(c, tmo, nop)) return;
     K::rebuild(app, a, 0, acc);
     K::flush_acc(a, acc, 0, 2);
-    if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, [&] { K::leader_start(app, a); })) return;
+    if (!grid_sync(c, tmo, [&] { K::leader_start(a, ps); })) return;
 
     WarpLB<TB> &my_lb = wlb[dev::warp_id()];
+    const int lb_push = a.p.lb_push, lb_pull = a.p.lb_pull;
     for (;;) {
         K::load_snap(a, s);
         if (s.done) break;
         const int var = s.variant;
         K::set_app_variant(app, var);
-        const int lb_push = a.p.lb_push, lb_pull = a.p.lb_pull;
         switch (var) {
             case V_ASYNC_PUSH_DD: {
                 K::clear_dirty(a, s);
                 K::push_phase_a(app, a, s, my_lb, true, lb_push, acc);
                 if (s.heavy_expected > 0 && lb_push != LB_NONE) {
                     K::flush_acc(a, acc, s.qhi, s.qlo);
-                    if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, nop)) return;
+                    if (!grid_sync(c, tmo, nop)) return;
                     K::heavy_phase(app, a, s, true, acc);
                 }
                 K::flush_acc(a, acc, s.qhi, s.qlo);
@@ -844,11 +1006,11 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
                 K::release_input_flags(a, s, false);
                 K::push_phase_a(app, a, s, my_lb, false, lb_push, acc);
                 K::flush_acc(a, acc, s.qhi, s.qlo);
-                if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, nop)) return;
+                if (!grid_sync(c, tmo, nop)) return;
                 if (lb_push != LB_NONE) {
                     K::heavy_phase(app, a, s, false, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
-                    if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, nop)) return;
+                    if (!grid_sync(c, tmo, nop)) return;
                 }
                 K::rebuild(app, a, s.qhi, acc);
                 K::flush_acc(a, acc, s.qhi, s.qlo);
@@ -859,15 +1021,23 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
             case V_SYNC_PULL_TD: {
                 const bool dd = is_dd(var);
                 const bool sync = is_sync(var);
-                const bool convert = dd && !(s.last_variant >= 0 && is_dd(s.last_variant) && is_pull(s.last_variant));
+                const bool convert = dd && !is_pull_dd(s.last_variant);
+                constexpr bool reduce = has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value;
                 K::clear_dirty(a, s);
                 K::release_input_flags(a, s, convert);
                 K::combine_all(app, a, sync);
-                if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, nop)) return;
-                K::pull_phase(app, a, s, dd, sync, lb_pull, acc);
+                if (!grid_sync(c, tmo, nop)) return;
+                if (reduce && !dd && lb_pull != LB_NONE) {
+                    K::pull_reduce_td(app, a, s, my_lb, acc);
+                    K::flush_acc(a, acc, s.qhi, s.qlo);
+                    if (!grid_sync(c, tmo, nop)) return;
+                    K::pull_reduce_chunks(app, a, acc);
+                } else {
+                    K::pull_phase(app, a, s, dd, sync, lb_pull, acc);
+                }
                 K::flush_acc(a, acc, s.qhi, s.qlo);
                 if (!dd) {
-                    if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, nop)) return;
+                    if (!grid_sync(c, tmo, nop)) return;
                     K::rebuild(app, a, s.qhi, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                 }
@@ -876,8 +1046,11 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
             default:
                 break;  // unsupported variants never start a round (leader_start / leader_end_round)
         }
-        if (!dev::grid_barrier(&c->bar_count, &c->bar_gen, &c->error, tmo, [&] { K::leader_end_round(app, a); }))
-            return;
+        if (!grid_sync(c, tmo, [&] { K::leader_end_round(app, a, ps); })) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c->edges_processed = dev::ld_l2(&c->cnt.edges_processed);
+        c->error = dev::ld_l2(&c->cnt.error);
     }
 }
 

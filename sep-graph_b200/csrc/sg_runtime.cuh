@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -27,6 +28,7 @@ struct sg_ctx {
     // pinned host staging for control-block read-back
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
+    int live_graphs = 0;  // sg_destroy refuses while graphs of this context exist
 };
 
 namespace sgb {
@@ -146,6 +148,7 @@ struct EngineConfig {
     double alpha = 15, beta = 18, edge_factor = 1.0;
     unsigned long long prio_init_raw = 0, prio_step_raw = 0;
     double timeout_s = 30.0;
+    int blocks_per_sm = 0;
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -154,7 +157,17 @@ struct EngineConfig {
 struct EngineResult {
     sepgraph::engine::Ctrl ctrl{};
     float ms = 0.f;
+    uint32_t grid_blocks = 0;
+    uint32_t device_error() const { return ctrl.error | ctrl.cnt.error; }
 };
+
+// Resident blocks per SM when the caller does not choose: small graphs are
+// bound by per-round barrier latency, which grows with the number of blocks.
+inline int auto_blocks_per_sm(uint32_t nv, uint64_t ne) {
+    if (ne < (1ull << 22)) return 2;
+    if (ne < (1ull << 25)) return 4;
+    return 8;
+}
 
 inline cudaError_t pinned(sg_ctx *ctx, size_t bytes, void **out) {
     if (ctx->pinned_bytes < bytes) {
@@ -244,15 +257,18 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     app.m_csc_graph = a.csc;
     app.m_nnodes = nv;
     app.m_nedges = (uint32_t)ne;
-    app.m_p_current_round = &a.ctrl->round;
+    app.m_p_current_round = &a.ctrl->rs.round;
 
     auto kernel = hybrid_engine_kernel<App, TV, TB, TW>;
-    static int blocks_per_sm = 0;  // one per template instantiation
-    if (blocks_per_sm == 0) {
-        SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kernel, kBlockThreads, 0));
-        if (blocks_per_sm <= 0) return set_error(ctx, SG_ERR_NO_DEVICE, "engine kernel cannot be resident");
+    static int max_blocks_per_sm = 0;  // one per template instantiation
+    if (max_blocks_per_sm == 0) {
+        SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks_per_sm, kernel, kBlockThreads, 0));
+        if (max_blocks_per_sm <= 0) return set_error(ctx, SG_ERR_NO_DEVICE, "engine kernel cannot be resident");
     }
-    dim3 grid(ctx->prop.multiProcessorCount * blocks_per_sm), block(kBlockThreads);
+    int bps = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : auto_blocks_per_sm(nv, ne);
+    bps = std::max(1, std::min(bps, max_blocks_per_sm));
+    dim3 grid(ctx->prop.multiProcessorCount * bps), block(kBlockThreads);
+    res->grid_blocks = grid.x;
 
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
@@ -273,8 +289,8 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
         std::memcpy(cfg.trace_out, (char *)h + sizeof(Ctrl),
                     sizeof(sg_round_trace) * std::min<uint32_t>(res->ctrl.n_trace, cfg.trace_cap));
     SG_TRY_CUDA(ctx, cudaEventElapsedTime(&res->ms, ctx->ev0, ctx->ev1));
-    const sg_status st = device_error_status(res->ctrl.error);
-    if (st != SG_OK) return set_error(ctx, st, "device error bits 0x%x", res->ctrl.error);
+    const sg_status st = device_error_status(res->device_error());
+    if (st != SG_OK) return set_error(ctx, st, "device error bits 0x%x", res->device_error());
     return SG_OK;
 }
 
@@ -285,9 +301,9 @@ inline void fill_stats(sg_stats *s, const EngineResult &r) {
     for (int i = 0; i < 8; ++i) s->rounds_by_variant[i] = r.ctrl.rounds_by_variant[i];
     s->time_kernel_ms = r.ms;
     s->time_total_ms = r.ms;
-    s->edges_processed = r.ctrl.edges_processed;
+    s->edges_processed = r.ctrl.cnt.edges_processed;
     s->vertices_processed = r.ctrl.vertices_processed;
-    s->device_error = r.ctrl.error;
+    s->device_error = r.device_error();
     s->n_trace = s->trace ? std::min<uint32_t>(r.ctrl.n_trace, s->trace_capacity) : 0;
 }
 

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from typing import Optional
 
 import numpy as np
@@ -50,7 +51,8 @@ class Options(C.Structure):
         ("priority_delta", C.c_double), ("cut_threshold", C.c_double), ("alpha", C.c_double),
         ("beta", C.c_double), ("edge_factor", C.c_double), ("max_iteration", C.c_int32), ("fused", C.c_int32),
         ("block_size", C.c_int32), ("non_atomic", C.c_int32), ("trace", C.c_int32), ("pr_error", C.c_double),
-        ("timeout_s", C.c_double), ("blocking", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("timeout_s", C.c_double), ("blocking", C.c_int32), ("blocks_per_sm", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -115,6 +117,7 @@ def load() -> C.CDLL:
         "sg_hgraph_gen_rmat": (C.c_int, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                          C.c_uint64, C.c_uint32, C.POINTER(_P)]),
         "sg_hgraph_gen_grid": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
+        "sg_hgraph_gen_random": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(_P)]),
         "sg_hgraph_from_csr": (C.c_int, [C.c_uint32, C.c_uint64, _P, _P, _P, C.POINTER(_P)]),
         "sg_hgraph_gen_weights": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint64]),
         "sg_hgraph_read_gr": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
@@ -193,6 +196,12 @@ class HostGraph:
     def grid(cls, rows: int, cols: int) -> "HostGraph":
         h = _P()
         _check(load().sg_hgraph_gen_grid(rows, cols, 0, C.byref(h)), "gen_grid")
+        return cls(h)
+
+    @classmethod
+    def random(cls, nv: int, gen_factor: int, seed: int = 1) -> "HostGraph":
+        h = _P()
+        _check(load().sg_hgraph_gen_random(nv, gen_factor, seed, C.byref(h)), "gen_random")
         return cls(h)
 
     @classmethod
@@ -284,6 +293,7 @@ class Context:
 
     def __init__(self, device: int = 0):
         self._c = _P()
+        self._graphs = weakref.WeakSet()
         _check(load().sg_init(device, C.byref(self._c)), "sg_init")
         self.device = device
 
@@ -315,16 +325,24 @@ class Context:
         _check(load().sg_graph_create_from_host(self._c, hg._h, flags, C.byref(g)), "graph_create", self._c)
         return Graph(self, g)
 
-    def graph_from_csr(self, offsets, indices, weights=None, symmetric=False, no_csc=False) -> "Graph":
+    def graph_from_csr(self, offsets, indices, weights=None, symmetric=False, no_csc=False, nv=None,
+                       ne=None) -> "Graph":
+        """Arrays may be numpy (host), torch tensors, or raw int pointers (then pass nv and ne)."""
         g = _P()
         flags = (GRAPH_SYMMETRIC if symmetric else 0) | (GRAPH_NO_CSC if no_csc else 0)
-        nv = (len(offsets) - 1) if not isinstance(offsets, int) else None
-        _check(load().sg_graph_create(self._c, nv, len(indices), _ptr(offsets), _ptr(indices), _ptr(weights),
-                                      flags, C.byref(g)), "graph_create", self._c)
+        if nv is None:
+            nv = len(offsets) - 1
+        if ne is None:
+            ne = len(indices)
+        _check(load().sg_graph_create(self._c, nv, ne, _ptr(offsets), _ptr(indices), _ptr(weights), flags,
+                                      C.byref(g)), "graph_create", self._c)
         return Graph(self, g)
 
     def close(self):
+        """Releases the context; graphs still open on it are released first."""
         if self._c:
+            for g in list(self._graphs):
+                g.close()
             load().sg_destroy(self._c)
             self._c = None
 
@@ -341,6 +359,7 @@ class Graph:
     def __init__(self, ctx: Context, handle):
         self.ctx = ctx
         self._g = handle
+        ctx._graphs.add(self)
 
     @property
     def handle(self):

@@ -166,6 +166,45 @@ def test_no_device_reports_status_not_crash():
     assert e.value.status == 8
 
 
+BIN = os.path.join(ROOT, "sep-graph_b200", "bin")
+# gflags names of the reference samples: app_skeleton.h:42-87 plus each sample's DEFINEs
+COMMON_FLAGS = {"interactive", "cmdfile", "max_iteration", "priority", "prio_delta", "edge_factor", "alpha", "beta",
+                "output", "check", "verbose", "trace", "lb_push", "lb_pull", "graphfile", "format", "undirected",
+                "json", "stats", "gen_graph", "gen_nnodes", "gen_factor", "gen_method", "gen_weights",
+                "gen_weight_range", "block_size", "grid_size", "wl_alloc_factor", "wl_sort", "wl_unique"}
+SAMPLE_FLAGS = {
+    "hybrid_bfs": {"source_node", "sparse", "variant", "non_atomic"},
+    "hybrid_sssp": {"source_node", "sparse", "variant"},
+    "hybrid_pr": {"cut_threshold", "sparse", "variant", "error", "top_ranks", "print_ranks", "norm"},
+    "hybrid_bc": {"source_node", "sparse", "src"},
+}
+
+
+@pytest.mark.parametrize("sample", sorted(SAMPLE_FLAGS))
+def test_cli_flag_surface(sample):
+    exe = os.path.join(BIN, sample)
+    if not os.path.exists(exe):
+        pytest.skip("samples not built")
+    out = subprocess.run([exe, "--help"], capture_output=True, text=True, timeout=30)
+    assert out.returncode == 0
+    names = set(re.findall(r"^\s+--(\w+)", out.stdout, re.M))
+    missing = (COMMON_FLAGS | SAMPLE_FLAGS[sample]) - names
+    assert not missing, missing
+    bad = subprocess.run([exe, "--no_such_flag=1"], capture_output=True, text=True, timeout=30)
+    assert bad.returncode != 0 and "unknown command line flag" in bad.stderr
+    bad = subprocess.run([exe, "--max_iteration=abc"], capture_output=True, text=True, timeout=30)
+    assert bad.returncode != 0 and "illegal value" in bad.stderr
+
+
+def test_random_generator_shape():
+    h = sg.HostGraph.random(2000, 10, seed=4)
+    deg = np.diff(h.offsets)
+    assert deg.min() >= 1 and deg.max() <= 10
+    src = np.repeat(np.arange(h.nv), deg)
+    assert not (src == h.indices).any() and _rows_sorted_unique(h.offsets, h.indices)
+    assert (sg.HostGraph.random(2000, 10, seed=4).indices == h.indices).all()
+
+
 def test_options_defaults_match_reference_flags():
     o = sg.make_options()
     assert o.alpha == 15 and o.beta == 18 and o.max_iteration == 200  # app_skeleton.h:44-51
