@@ -46,7 +46,39 @@ def args_parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--all", action="store_true")
     p.add_argument("--scale", type=int, default=SCALE)
+    p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc"],
+                   help="run one warm-up and one measured solve of that kernel only (for ncu captures)")
     return p.parse_args()
+
+
+def run_profile(a):
+    """Two solves of one engine instantiation (the second is the one to capture)."""
+    import sepgraph as sg
+
+    ctx = sg.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    sym = a.profile in ("bfs", "bc")
+    h = sg.HostGraph.rmat(a.scale, EDGE_FACTOR, 0.57, 0.19, 0.19, seed=1, symmetric=sym)
+    if a.profile.startswith("sssp"):
+        h.gen_weights(1, 64, 2)
+    G = ctx.graph(h, symmetric=sym)
+    src = h.max_degree_vertex()[0] if sym else int(h.pick_sources(1, 3)[0])
+    for _ in range(2):
+        if a.profile == "sssp_push":
+            _, st, _ = G.sssp(src, variant="async_push_dd", max_iteration=100000)
+        elif a.profile == "sssp_delta":
+            _, st, _ = G.sssp(src, priority="low_high", max_iteration=1000000)
+        elif a.profile == "bfs":
+            _, st, _ = G.bfs(src)
+        elif a.profile == "pr_pull":
+            _, st, _ = G.pagerank(variant="sync_pull_td", pr_error=1e-7, max_iteration=1000)
+        elif a.profile == "pr_push":
+            _, st, _ = G.pagerank(variant="async_push_dd", pr_error=1e-7, max_iteration=1000)
+        else:
+            _, _, st = G.bc(src)
+        print(json.dumps({"profile": a.profile, "scale": a.scale, "ms": st.time_kernel_ms, "rounds": st.rounds,
+                          "edges_reached": st.edges_reached, "edges_processed": st.edges_processed}), flush=True)
+    G.close()
+    ctx.close()
 
 
 def peak_hbm():
@@ -374,7 +406,9 @@ def run_all(ctx, torch):
 
 def main():
     a = args_parse()
-    if a.impl == "reference":
+    if a.profile:
+        run_profile(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

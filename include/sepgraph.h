@@ -89,7 +89,9 @@ typedef struct sg_options {
     double timeout_s;         /* bound on any device-side wait; 0 = default (30 s) */
     int32_t blocking;         /* 1: wait and fill sg_stats (default); 0: enqueue only */
     int32_t blocks_per_sm;    /* resident engine blocks per SM; 0 = library choice by graph size */
-    int32_t reserved[6];
+    int32_t heavy_degree;     /* push/pull: vertices above this many edges are split into chunks; 0 = 32 */
+    int32_t chunk_edges;      /* edges per chunk of a split vertex; 0 = 256 */
+    int32_t reserved[4];
 } sg_options;
 
 /* Per-round trace record (the reference's --trace line, framework.cuh:334-348). */

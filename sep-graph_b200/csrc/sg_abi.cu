@@ -64,8 +64,8 @@ __global__ void reached_stats_kernel(const uint32_t *row, const uint32_t *value,
 // Each vertex is owned by one thread (small out-degree) or one warp; vertices
 // above kBcBigDegree out-edges are split into chunks whose partial sums are
 // added atomically after a barrier.  The source (depth 0) keeps delta 0.
-constexpr uint32_t kBcBigDegree = 2048;
-constexpr uint32_t kBcChunk = 2048;
+constexpr uint32_t kBcBigDegree = 256;
+constexpr uint32_t kBcChunk = 256;
 
 struct BCBackArgs {
     const uint32_t *row, *col;
@@ -200,6 +200,8 @@ sgb::EngineConfig make_config(const sg_graph *g, const sg_options &o, int scheme
     if (o.alpha == 0) c.forced = engine::V_ASYNC_PUSH_DD;  // framework.cuh:445-448
     c.timeout_s = o.timeout_s;
     c.blocks_per_sm = o.blocks_per_sm;
+    if (o.heavy_degree > 0) c.heavy_degree = (uint32_t)o.heavy_degree;
+    if (o.chunk_edges > 0) c.chunk_edges = (uint32_t)o.chunk_edges;
     c.blocking = o.blocking != 0;
     if (o.trace && stats && stats->trace && stats->trace_capacity) {
         c.trace = 1;

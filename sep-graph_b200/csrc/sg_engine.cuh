@@ -132,7 +132,7 @@ struct KArgs {
     uint32_t *queue[3];
     uint32_t queue_cap;
     uint32_t *bitmap[2];
-    uint32_t *qflag[2];
+    uint32_t *qflag[3];  // queued bitmap of each worklist slot
     uint32_t nwords;
     uint32_t *middle;
     HeavyItem<TBuffer> *heavy;
@@ -310,18 +310,22 @@ struct EngineKernel {
         acc.reset();
     }
 
-    // Append dst to the next worklist(s) if `want`: dedupe through the queued
-    // bitmap, route by IsHighPriority when two-level priority is on, and count
-    // its out-degree for the policy.  All 32 lanes must call.
+    // Append dst to the next worklist(s) if `want`: dedupe through the output
+    // slot's queued bitmap, route by IsHighPriority when two-level priority is
+    // on, and count its out-degree for the policy.  Each worklist slot has its
+    // own queued bitmap: pops clear bits of the input slot only and appends set
+    // bits of an output slot only, so a vertex improved during a round always
+    // reaches the next round's worklist (which reads it after the barrier) and
+    // no fence is needed between the state update and the queued bit.
+    // All 32 lanes must call.
     static __device__ __forceinline__ void enqueue(App &app, const Args &a, const Snap &s, uint32_t dst, bool want,
                                                    Acc &acc) {
         Counters *n = &a.ctrl->cnt;
         bool hi = true;
         if (a.p.priority && want) hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), dev::ld_l2(a.buffer + dst));
         bool w_hi = want && hi, w_lo = want && !hi;
-        if (want) __threadfence();  // order the buffer update before publishing the queued bit
-        if (w_hi) w_hi = dev::bitmap_set(a.qflag[0], dst);
-        if (w_lo) w_lo = dev::bitmap_set(a.qflag[1], dst);
+        if (w_hi) w_hi = dev::bitmap_set(a.qflag[s.qhi], dst);
+        if (w_lo) w_lo = dev::bitmap_set(a.qflag[s.qlo], dst);
         dev::warp_append(a.queue[s.qhi], &n->qcount[s.qhi], a.queue_cap, w_hi, dst, &n->error);
         if (a.p.priority) dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, w_lo, dst, &n->error);
         if (w_hi || w_lo) acc.count(w_hi, out_degree(a, dst), a.p.heavy_threshold);
@@ -333,10 +337,8 @@ struct EngineKernel {
         Counters *n = &a.ctrl->cnt;
         bool hi = true;
         if (a.p.priority) hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), dev::ld_l2(a.buffer + dst));
-        __threadfence();
-        const int k = hi ? 0 : 1;
-        if (!dev::bitmap_set(a.qflag[k], dst)) return;
         const uint32_t q = hi ? s.qhi : s.qlo;
+        if (!dev::bitmap_set(a.qflag[q], dst)) return;
         const uint32_t pos = atomicAdd(&n->qcount[q], 1u);
         if (pos < a.queue_cap)
             a.queue[q][pos] = dst;
@@ -345,22 +347,38 @@ struct EngineKernel {
         acc.count(hi, out_degree(a, dst), a.p.heavy_threshold);
     }
 
-    static __device__ __forceinline__ void register_heavy(const Args &a, uint32_t src, uint32_t beg, uint32_t deg,
-                                                          TB payload) {
+    // Registers the lanes' heavy vertices as chunk lists (warp-aggregated: one
+    // ballot, one scan, two atomics per warp).  All 32 lanes must call.
+    static __device__ __forceinline__ void register_heavy(const Args &a, bool heavy, uint32_t src, uint32_t beg,
+                                                          uint32_t deg, TB payload) {
+        const uint32_t m = __ballot_sync(dev::kFullMask, heavy);
+        if (m == 0) return;
         Counters *n = &a.ctrl->cnt;
+        const uint32_t lane = dev::lane_id();
         const uint32_t ce = a.p.chunk_edges;
-        const uint32_t nch = (deg + ce - 1) / ce;
-        const uint32_t idx = atomicAdd(&n->heavy_count, 1u);
-        const uint32_t cb = atomicAdd(&n->chunk_count, nch);
-        if (idx < a.heavy_cap && cb <= a.chunk_cap && nch <= a.chunk_cap - cb) {
+        const uint32_t nch = heavy ? (deg + ce - 1) / ce : 0u;
+        const uint32_t incl = dev::warp_inclusive_scan(nch);
+        const uint32_t tot = __shfl_sync(dev::kFullMask, incl, 31);
+        const uint32_t leader = __ffs(m) - 1;
+        uint32_t hb = 0, cb = 0;
+        if (lane == leader) {
+            hb = atomicAdd(&n->heavy_count, (uint32_t)__popc(m));
+            cb = atomicAdd(&n->chunk_count, tot);
+        }
+        hb = __shfl_sync(dev::kFullMask, hb, leader);
+        cb = __shfl_sync(dev::kFullMask, cb, leader);
+        if (!heavy) return;
+        const uint32_t idx = hb + __popc(m & dev::lanemask_lt());
+        const uint32_t c0 = cb + incl - nch;
+        if (idx < a.heavy_cap && c0 <= a.chunk_cap && nch <= a.chunk_cap - c0) {
             HeavyItem<TB> h;
             h.src = src;
             h.beg = beg;
             h.deg = deg;
-            h.chunk_base = cb;
+            h.chunk_base = c0;
             h.payload = payload;
             a.heavy[idx] = h;
-            for (uint32_t i = 0; i < nch; ++i) a.chunk_owner[cb + i] = idx;
+            for (uint32_t i = 0; i < nch; ++i) a.chunk_owner[c0 + i] = idx;
         } else {
             atomicOr(&n->error, dev::kErrChunkCapacity);
         }
@@ -467,7 +485,7 @@ struct EngineKernel {
         const uint32_t *Q = a.queue[s.qin];
         for (uint32_t i = gthread(); i < s.F; i += nthreads()) {
             const uint32_t v = dev::ld_l2(Q + i);
-            dev::bitmap_clear(a.qflag[0], v);
+            dev::bitmap_clear(a.qflag[s.qin], v);
             if (to_bitmap) dev::bitmap_set(a.bitmap[s.bin], v);  // Queue2Bitmap (driver.cuh:119-129)
         }
     }
@@ -490,22 +508,16 @@ struct EngineKernel {
             if (valid) {
                 v = dd ? dev::ld_l2(Q + i) : i;
                 if (dd) {
-                    if (s.pile) {
-                        // far pile: vertices still outside the priority window stay in the pile
-                        if (!app.App::IsHighPriority(prio, dev::ld_l2(a.buffer + v))) {
-                            keep = true;
-                            proceed = false;
-                        } else {
-                            dev::bitmap_clear(a.qflag[1], v);
-                        }
-                    } else {
-                        dev::bitmap_clear(a.qflag[0], v);
+                    dev::bitmap_clear(a.qflag[s.qin], v);  // pop
+                    if (s.pile && !app.App::IsHighPriority(prio, dev::ld_l2(a.buffer + v))) {
+                        // far pile: vertices still outside the priority window move to the new pile
+                        keep = dev::bitmap_set(a.qflag[s.qlo], v);
+                        proceed = false;
                     }
                 }
             }
-            if (dd) {
-                __threadfence();  // pop (queued bit cleared) before reading the vertex state
-                if (s.pile) dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, keep, v, &n->error);
+            if (dd && s.pile) {
+                dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, keep, v, &n->error);
                 if (keep) acc.count(false, out_degree(a, v), a.p.heavy_threshold);
             }
             TB payload{};
@@ -524,10 +536,9 @@ struct EngineKernel {
                 if (deg) expand_serial(app, a, s, v, beg, deg, payload, dd, acc);
                 continue;
             }
-            if (deg > a.p.heavy_threshold) {
-                register_heavy(a, v, beg, deg, payload);
-                deg = 0;
-            }
+            const bool heavy = deg > a.p.heavy_threshold;
+            register_heavy(a, heavy, v, beg, deg, payload);
+            if (heavy) deg = 0;
             expand_warp(app, a, s, wlb, v, beg, deg, payload, dd, acc);
         }
     }
@@ -634,9 +645,8 @@ struct EngineKernel {
             if (dd) {
                 bool want = valid && hit;
                 if (want) {
-                    __threadfence();
                     dev::bitmap_set(a.bitmap[s.bout], v);
-                    want = dev::bitmap_set(a.qflag[0], v);
+                    want = dev::bitmap_set(a.qflag[s.qhi], v);
                 }
                 dev::warp_append(a.queue[s.qhi], &n->qcount[s.qhi], a.queue_cap, want, v, &n->error);
                 if (want) acc.count(true, out_degree(a, v), a.p.heavy_threshold);
@@ -661,10 +671,9 @@ struct EngineKernel {
                     beg = a.csc.begin_edge(v);
                     deg = a.csc.end_edge(v) - beg;
                 }
-                if (deg > a.p.heavy_threshold) {
-                    register_heavy(a, v, beg, deg, app.PullIdentity());
-                    deg = 0;
-                }
+                const bool heavy = deg > a.p.heavy_threshold;
+                register_heavy(a, heavy, v, beg, deg, app.PullIdentity());
+                if (heavy) deg = 0;
                 const uint32_t incl = dev::warp_inclusive_scan(deg);
                 const uint32_t total = __shfl_sync(dev::kFullMask, incl, 31);
                 w.excl[lane] = incl - deg;
@@ -734,7 +743,7 @@ struct EngineKernel {
             const uint32_t v = base + lane;
             bool act = false;
             if (v < N) act = app.App::IsActiveNode(v, dev::ld_l2(a.buffer + v));
-            if (act) act = dev::bitmap_set(a.qflag[0], v);
+            if (act) act = dev::bitmap_set(a.qflag[slot], v);
             dev::warp_append(a.queue[slot], &n->qcount[slot], a.queue_cap, act, v, &n->error);
             if (act) acc.count(true, out_degree(a, v), a.p.heavy_threshold);
         }
@@ -976,6 +985,7 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
         a.bitmap[1][w] = 0;
         a.qflag[0][w] = 0;
         a.qflag[1][w] = 0;
+        a.qflag[2][w] = 0;
     }
     if (!grid_sync(c, tmo, nop)) return;
     K::rebuild(app, a, 0, acc);

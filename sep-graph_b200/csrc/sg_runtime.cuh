@@ -149,6 +149,8 @@ struct EngineConfig {
     unsigned long long prio_init_raw = 0, prio_step_raw = 0;
     double timeout_s = 30.0;
     int blocks_per_sm = 0;
+    uint32_t heavy_degree = 32;  // out/in-degree above which a vertex is split into chunks
+    uint32_t chunk_edges = 256;
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -209,9 +211,14 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     a.buffer = buffer;
 
     const uint32_t nwords = (nv + 31) / 32 + 1;
-    const uint32_t heavy_threshold = 1024, chunk_edges = 1024;
-    const uint32_t heavy_cap = (uint32_t)(ne / heavy_threshold + 2);
-    const uint32_t chunk_cap = (uint32_t)(ne / chunk_edges + ne / heavy_threshold + 2);
+    // A warp task is 32 light vertices (<= heavy_threshold edges each) or one
+    // chunk of a heavy vertex (<= chunk_edges), which bounds the slowest warp
+    // of a round.  Each vertex is registered at most once per round, so the
+    // tables are bounded by the vertices above the threshold.
+    const uint32_t heavy_threshold = std::max<uint32_t>(1, cfg.heavy_degree);
+    const uint32_t chunk_edges = std::max<uint32_t>(32, cfg.chunk_edges);
+    const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(nv, ne / heavy_threshold) + 2;
+    const uint32_t chunk_cap = (uint32_t)(ne / chunk_edges + heavy_cap + 2);
     auto &ws = g->ws;
     SG_TRY_CUDA(ctx, ws.get("tmp", nv, &a.tmp));
     SG_TRY_CUDA(ctx, ws.get("q0", nv, &a.queue[0]));
@@ -221,6 +228,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     SG_TRY_CUDA(ctx, ws.get("bm1", nwords, &a.bitmap[1]));
     SG_TRY_CUDA(ctx, ws.get("fl0", nwords, &a.qflag[0]));
     SG_TRY_CUDA(ctx, ws.get("fl1", nwords, &a.qflag[1]));
+    SG_TRY_CUDA(ctx, ws.get("fl2", nwords, &a.qflag[2]));
     SG_TRY_CUDA(ctx, ws.get("middle", nv, &a.middle));
     SG_TRY_CUDA(ctx, ws.get("heavy", heavy_cap, &a.heavy, true));
     SG_TRY_CUDA(ctx, ws.get("chunk", chunk_cap, &a.chunk_owner, true));

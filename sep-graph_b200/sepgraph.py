@@ -52,7 +52,7 @@ class Options(C.Structure):
         ("beta", C.c_double), ("edge_factor", C.c_double), ("max_iteration", C.c_int32), ("fused", C.c_int32),
         ("block_size", C.c_int32), ("non_atomic", C.c_int32), ("trace", C.c_int32), ("pr_error", C.c_double),
         ("timeout_s", C.c_double), ("blocking", C.c_int32), ("blocks_per_sm", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("heavy_degree", C.c_int32), ("chunk_edges", C.c_int32), ("reserved", C.c_int32 * 4),
     ]
 
 
