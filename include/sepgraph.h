@@ -163,6 +163,23 @@ sg_status sg_pagerank(sg_graph *g, const sg_options *opt, float *ranks_out, floa
 sg_status sg_bc(sg_graph *g, uint32_t source, const sg_options *opt, float *bc_out, uint64_t *sigma_out,
                 sg_stats *stats);
 
+/* BFS that allocates nothing, for callers that cannot call cudaMalloc (code
+ * running inside another framework's memory pool or under a device-memory
+ * budget).  No counterpart in the reference.  Runs the sg_bfs engine on the
+ * calling thread's current device with every worklist, bitmap and control word
+ * in one fixed file-scope device array (about 13 MB, held by every GPU that
+ * loads it until exit).  Limits: nv <= 262144 vertices, ne <= 8388608 edges;
+ * larger graphs return SG_ERR_CAPACITY before any work.  offsets/indices (CSR),
+ * optional in_offsets/in_indices (CSC; pass the CSR again for a symmetric
+ * graph, NULL for push-only) and levels_out are device memory of the current
+ * device.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Calls share the array: calls that overlap on the
+ * GPU race.  Blocks until done; err (optional) receives a message. */
+sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *indices, uint32_t nv, uint64_t ne,
+                         const uint32_t *in_offsets, const uint32_t *in_indices, uint32_t source,
+                         const sg_options *opt, uint32_t *levels_out, void *cuda_stream, sg_stats *stats, char *err,
+                         size_t err_len);
+
 /* ------------------------------------------------------------------ host graphs (ingest)
  * Seeded generators (the reference's generators are unseeded, traversal.h:173-189)
  * and Galois .gr I/O (src/utils/parser.cpp:409-506). */
