@@ -253,9 +253,9 @@ def run_ours(a):
     modes = {"hybrid": dict(max_iteration=100000), "push_dd": dict(variant="async_push_dd", max_iteration=100000)}
     avg_w = float(h.weights.mean())
     base_delta = max(1, int(32 * avg_w / (ne / nv)))
-    for mult in (1, 2, 4, 8):
-        modes[f"delta{base_delta * mult}"] = dict(priority="low_high", priority_delta=base_delta * mult,
-                                                  max_iteration=1000000)
+    for div in (16, 8, 4, 2, 1):  # around the reference heuristic 32*avg_w/avg_deg (hybrid_sssp.cu:196-197)
+        d = max(1, base_delta // div)
+        modes[f"delta{d}"] = dict(priority="low_high", priority_delta=d, max_iteration=1000000)
     e_reached, mode_ms, ref0 = {}, {}, None
     for name, kw in modes.items():
         ts = []

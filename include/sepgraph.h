@@ -65,7 +65,10 @@ enum {
 };
 
 /* Graph creation flags. */
-#define SG_GRAPH_SYMMETRIC 0x1u  /* CSC aliases CSR (reference --undirected, csr_graph.h:405-410) */
+/* CSC aliases CSR (reference --undirected, csr_graph.h:405-410).  With weights,
+ * per-edge weights that differ between u->v and v->u get their own CSC weight
+ * array (the reference would pull the reverse edge's weight). */
+#define SG_GRAPH_SYMMETRIC 0x1u
 #define SG_GRAPH_NO_CSC 0x2u     /* do not build the in-edge (CSC) view; pull variants then fail */
 
 /* Engine options: union of EngineOptions (common.h:203-321) and the flags the
@@ -162,6 +165,95 @@ sg_status sg_pagerank(sg_graph *g, const sg_options *opt, float *ranks_out, floa
  * like hybrid_bc.cu:374-376. sigma_out optional (uint64 path counts). */
 sg_status sg_bc(sg_graph *g, uint32_t source, const sg_options *opt, float *bc_out, uint64_t *sigma_out,
                 sg_stats *stats);
+
+/* ------------------------------------------------------------------ batching
+ * No counterpart in the reference (one source per Engine).  Multi-source BFS:
+ * up to 64 sources in one persistent launch with 64-bit per-vertex source
+ * masks.  levels_out holds nsrc rows of nv uint32 (row i = BFS from
+ * sources[i], identical to sg_bfs from that source). */
+sg_status sg_msbfs(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt, uint32_t *levels_out,
+                   sg_stats *stats);
+
+/* sg_msbfs on a chosen context (stream and scratch of ctx; the graph may belong
+ * to another context of the same device). */
+sg_status sg_msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt,
+                      uint32_t *levels_out, sg_stats *stats);
+
+/* One query of a batch: graph (any graph of the context), source, and the
+ * output array of graph->nv uint32 (host or device memory). */
+typedef struct sg_batch_query {
+    sg_graph *graph;
+    uint32_t source;
+    uint32_t pad;
+    void *out;
+} sg_batch_query;
+
+/* Batched SSSP / BFS: n queries over any mix of graphs in ONE cooperative
+ * launch.  The grid is split into teams of blocks (sg_options.reserved[0] =
+ * blocks per team, 0 = by graph size); each team runs one query's whole round
+ * loop with its own frontiers and takes the next query (largest graphs first)
+ * when done.  Every output equals sg_sssp / sg_bfs for that query.  stats is
+ * the aggregate (time of the launch, summed reached edges);
+ * per_query_ms (optional, n floats) receives each query's device time. */
+sg_status sg_sssp_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt, sg_stats *stats,
+                        float *per_query_ms);
+sg_status sg_bfs_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt, sg_stats *stats,
+                       float *per_query_ms);
+
+/* Batched single-source BC: each team runs one query's hybrid forward pass and
+ * its backward dependency pass in the same launch; out receives graph->nv
+ * floats equal to sg_bc's bc_out for that source (path counts stay on the
+ * device).  stats->edges_reached counts both traversals, as sg_bc does. */
+sg_status sg_bc_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt, sg_stats *stats,
+                      float *per_query_ms);
+
+/* ------------------------------------------------------------------ serving
+ * No counterpart in the reference.  A query server over device-resident
+ * graphs with continuous batching: `slots` worker threads, each with its own
+ * context and stream, repeatedly take the pending queries of one algorithm
+ * (oldest first, up to max_batch), admit them against the HBM budget and run
+ * them as one batched launch (multi-source BFS per graph, sg_sssp_batch /
+ * sg_bfs_batch across graphs, one PageRank per graph shared by its queries,
+ * sg_bc_batch).  Queries that arrive while batches run are taken as soon as
+ * a slot frees; batches of different slots overlap on the device.  Every
+ * result equals the single-query call's. */
+typedef struct sg_server sg_server;
+enum { SG_QUERY_BFS = 0, SG_QUERY_SSSP = 1, SG_QUERY_PAGERANK = 2, SG_QUERY_BC = 3 };
+typedef struct sg_server_config {
+    uint64_t hbm_budget_bytes; /* admission budget for batch scratch and staging (0 = 1/4 of HBM) */
+    uint32_t slots;            /* concurrent batches (default 3) */
+    uint32_t max_batch;        /* queries per batch (default 256) */
+    uint32_t max_pending;      /* submit returns SG_ERR_BUSY beyond this (default 1<<20) */
+    uint32_t msbfs_min;        /* BFS queries of one graph that go to multi-source BFS (default 4) */
+    uint32_t sssp_delta;       /* 0: SSSP as ASYNC_PUSH_DD; >0: two-level priority with this delta */
+    uint32_t pad;
+    double pr_error;           /* PageRank residual threshold (default 1e-7) */
+    int32_t reserved[8];
+} sg_server_config;
+typedef struct sg_query {
+    int32_t algo;      /* SG_QUERY_* */
+    uint32_t graph_id; /* from sg_server_add_graph */
+    uint32_t source;   /* ignored by PageRank */
+    uint32_t pad;
+    void *out;         /* host buffer of nv elements: uint32 levels / distances, float ranks / bc */
+    void *out2;        /* BC: optional uint64 path counts */
+} sg_query;
+typedef struct sg_server_stats {
+    uint64_t submitted, completed, failed, batches, pending;
+    double elapsed_s; /* first submit to last completion */
+    double qps, mean_ms, p50_ms, p99_ms, p999_ms, max_ms;
+    uint64_t hbm_budget, hbm_in_use, hbm_peak;
+} sg_server_stats;
+sg_status sg_server_config_default(sg_server_config *cfg);
+sg_status sg_server_create(int device, const sg_server_config *cfg, sg_server **out);
+sg_status sg_server_add_graph(sg_server *s, sg_graph *g, uint32_t *graph_id);
+sg_status sg_server_submit(sg_server *s, const sg_query *q, uint64_t *ticket);
+/* Waits for one query; *result receives its status, *latency_ms submit-to-completion. */
+sg_status sg_server_wait(sg_server *s, uint64_t ticket, double timeout_s, sg_status *result, double *latency_ms);
+sg_status sg_server_drain(sg_server *s, double timeout_s);
+sg_status sg_server_get_stats(sg_server *s, sg_server_stats *st);
+sg_status sg_server_reset_stats(sg_server *s);
+sg_status sg_server_destroy(sg_server *s);
 
 /* BFS that allocates nothing, for callers that cannot call cudaMalloc (code
  * running inside another framework's memory pool or under a device-memory

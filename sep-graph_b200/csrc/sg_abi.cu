@@ -11,6 +11,7 @@
 
 #include "host/sg_hgraph.h"
 #include "sg_apps.cuh"
+#include "sg_bc.cuh"
 #include "sg_runtime.cuh"
 
 using namespace sepgraph;
@@ -56,104 +57,14 @@ __global__ void reached_stats_kernel(const uint32_t *row, const uint32_t *value,
 }
 
 // ---------------------------------------------------------------- BC backward
-// Dependency accumulation of Brandes' algorithm over the forward level stack,
-// deepest level first, one grid barrier per phase (StageTwoDD{,CTA}Fused,
-// samples/hybrid_bc/hybrid_bc.cu:134-225; host form hybrid_bc_host.cpp:66-80):
-//   delta[v] = sum over out-edges v->w with level[w] == level[v]+1 of
-//              sigma[v]/sigma[w] * (1 + delta[w])
-// Each vertex is owned by one thread (small out-degree) or one warp; vertices
-// above kBcBigDegree out-edges are split into chunks whose partial sums are
-// added atomically after a barrier.  The source (depth 0) keeps delta 0.
-constexpr uint32_t kBcBigDegree = 256;
-constexpr uint32_t kBcChunk = 256;
-
-struct BCBackArgs {
-    const uint32_t *row, *col;
-    const uint32_t *level;
-    const unsigned long long *sigma;
-    float *delta;
-    float *bc_out;  // delta * 0.5 (hybrid_bc.cu:374-376)
-    const uint32_t *stack, *ends;
-    uint32_t nlevels, max_depth, nv;
-    uint4 *chunks;  // (v, begin, len, -)
-    uint32_t chunk_cap;
-    uint32_t *chunk_count;  // [max_depth + 1]
-    uint32_t *bar;          // count, gen
-    uint32_t *err;
-    unsigned long long timeout_ns;
-};
-
-__device__ __forceinline__ float bc_term(const BCBackArgs &a, unsigned long long sv, uint32_t w, uint32_t d) {
-    if (__ldcg(a.level + w) != d + 1) return 0.f;
-    const float ratio = (float)((double)sv / (double)__ldcg(a.sigma + w));
-    return ratio * (1.0f + __ldcg(a.delta + w));
-}
+// One query over the whole cooperative grid (sg_bc.cuh has the pass itself).
+using bc::BCBackArgs;
+using bc::kBcBigDegree;
+using bc::kBcChunk;
 
 __global__ void __launch_bounds__(256) bc_backward_kernel(BCBackArgs a) {
-    const uint32_t lane = dev::lane_id();
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    auto nop = [] {};
-    for (uint32_t d = a.max_depth; d >= 1; --d) {
-        const uint32_t b = __ldcg(a.ends + d - 1), e = __ldcg(a.ends + d);
-        for (uint32_t base = b + gw * 32; base < e; base += nw * 32) {
-            const uint32_t i = base + lane;
-            const bool valid = i < e;
-            uint32_t v = 0, beg = 0, deg = 0;
-            unsigned long long sv = 0;
-            if (valid) {
-                v = __ldcg(a.stack + i);
-                beg = __ldg(a.row + v);
-                deg = __ldg(a.row + v + 1) - beg;
-                sv = __ldcg(a.sigma + v);
-            }
-            bool big = valid && deg > kBcBigDegree;
-            bool mid = valid && !big && deg > 32;
-            if (valid && !big && !mid) {
-                float s = 0.f;
-                for (uint32_t k = beg; k < beg + deg; ++k) s += bc_term(a, sv, __ldg(a.col + k), d);
-                a.delta[v] = s;
-            }
-            if (big) {
-                const uint32_t nch = (deg + kBcChunk - 1) / kBcChunk;
-                const uint32_t c0 = atomicAdd(a.chunk_count + d, nch);
-                for (uint32_t c = 0; c < nch; ++c) {
-                    if (c0 + c < a.chunk_cap)
-                        a.chunks[c0 + c] = make_uint4(v, beg + c * kBcChunk, min(kBcChunk, deg - c * kBcChunk), 0);
-                    else
-                        atomicOr(a.err, dev::kErrChunkCapacity);
-                }
-            }
-            uint32_t m = __ballot_sync(dev::kFullMask, mid);
-            while (m) {
-                const uint32_t j = __ffs(m) - 1;
-                m &= m - 1;
-                const uint32_t vj = __shfl_sync(dev::kFullMask, v, j);
-                const uint32_t bj = __shfl_sync(dev::kFullMask, beg, j);
-                const uint32_t dj = __shfl_sync(dev::kFullMask, deg, j);
-                const unsigned long long sj = __shfl_sync(dev::kFullMask, sv, j);
-                float s = 0.f;
-                for (uint32_t k = lane; k < dj; k += 32) s += bc_term(a, sj, __ldg(a.col + bj + k), d);
-                s = dev::warp_sum(s);
-                if (lane == 0) a.delta[vj] = s;
-            }
-        }
-        if (!dev::grid_barrier(a.bar, a.bar + 1, a.err, a.timeout_ns, nop)) return;
-        const uint32_t nc = min(__ldcg(a.chunk_count + d), a.chunk_cap);
-        if (nc) {
-            for (uint32_t c = gw; c < nc; c += nw) {
-                const uint4 ch = a.chunks[c];
-                const unsigned long long sv = __ldcg(a.sigma + ch.x);
-                float s = 0.f;
-                for (uint32_t k = lane; k < ch.z; k += 32) s += bc_term(a, sv, __ldg(a.col + ch.y + k), d);
-                s = dev::warp_sum(s);
-                if (lane == 0) atomicAdd(a.delta + ch.x, s);
-            }
-            if (!dev::grid_barrier(a.bar, a.bar + 1, a.err, a.timeout_ns, nop)) return;
-        }
-    }
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nv; v += gridDim.x * blockDim.x)
-        a.bc_out[v] = __ldcg(a.delta + v) * 0.5f;
+    auto sync = [&] { return dev::grid_barrier(a.bar, a.bar + 1, a.err, a.timeout_ns, [] {}); };
+    bc::backward(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, sync);
 }
 
 __global__ void bc_scale_kernel(const float *delta, float *out, uint32_t nv) {
@@ -309,6 +220,7 @@ sg_status sg_destroy(sg_ctx *ctx) {
     DeviceGuard dg(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    delete ctx->batch_ws;
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -398,15 +310,27 @@ sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t 
         for (uint64_t e = 0; e < ne; ++e) ws += w[e];
     g->weight_sum = w ? ws : (double)ne;
 
+    // A symmetric graph's CSC aliases its CSR (csr_graph.h:405-410).  With edge
+    // weights that alias is only right when w(u->v) == w(v->u) edge by edge, so
+    // a weighted symmetric graph is transposed: an identical structure is still
+    // aliased and only weights that differ get their own CSC weight array; a
+    // structure whose transpose lists neighbours in another order gets a full CSC.
     std::vector<uint32_t> coff, cidx, cw;
-    const bool build_csc = g->has_csc && !g->symmetric;
-    if (build_csc) sgb::transpose(nv, ne, off, idx, w, coff, cidx, cw);
+    bool build_csc = g->has_csc && !g->symmetric;
+    bool own_cw = false;
+    if (build_csc || (g->has_csc && w)) sgb::transpose(nv, ne, off, idx, w, coff, cidx, cw);
+    if (g->has_csc && g->symmetric && w) {
+        const bool same_structure = std::equal(coff.begin(), coff.end(), off) && std::equal(cidx.begin(), cidx.end(), idx);
+        build_csc = !same_structure;
+        own_cw = same_structure && !std::equal(cw.begin(), cw.end(), w);
+    }
 
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t b_row = al(4ull * (nv + 1)), b_col = al(4ull * std::max<uint64_t>(ne, 1));
     const size_t b_w = w ? b_col : 0;
     size_t total = b_row + b_col + b_w;
     if (build_csc) total += b_row + b_col + b_w;
+    if (own_cw) total += b_w;
     cudaError_t e = cudaMalloc(&g->arena, total);
     if (e != cudaSuccess) {
         delete g;
@@ -431,10 +355,14 @@ sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t 
             g->cw = (uint32_t *)p;
             p += b_w;
         }
-    } else if (g->has_csc) {  // symmetric: CSC aliases CSR (csr_graph.h:405-410)
+    } else if (g->has_csc) {  // symmetric: CSC aliases CSR
         g->crow = g->row;
         g->ccol = g->col;
         g->cw = g->w;
+        if (own_cw) {
+            g->cw = (uint32_t *)p;
+            p += b_w;
+        }
     }
     sg_status st = SG_OK;
     auto cp = [&](void *dst, const void *src, size_t bytes) {
@@ -450,6 +378,8 @@ sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t 
         cp(g->crow, coff.data(), 4ull * (nv + 1));
         cp(g->ccol, cidx.data(), 4ull * ne);
         if (w) cp(g->cw, cw.data(), 4ull * ne);
+    } else if (own_cw) {
+        cp(g->cw, cw.data(), 4ull * ne);
     }
     if (st != SG_OK) {
         cudaFree(g->arena);
@@ -476,6 +406,12 @@ sg_status sg_graph_destroy(sg_graph *g) {
     delete g;
     return SG_OK;
 }
+
+}  // extern "C"
+
+sg_ctx *sgb::graph_context(const sg_graph *g) { return g ? g->ctx : nullptr; }
+
+extern "C" {
 
 sg_status sg_graph_info(const sg_graph *g, uint32_t *nv, uint64_t *ne, uint64_t *device_bytes, int *weighted) {
     if (!g) return SG_ERR_INVALID_ARG;

@@ -1,0 +1,894 @@
+// Batched traversals: many BFS sources in one persistent launch.
+//
+// Multi-source BFS with 64-bit per-vertex source masks (bit i = source i).
+// Each round: expand the active vertices' masks to their neighbours (push,
+// atomicOr of the bits the neighbour has not seen) or let every vertex that
+// still misses some source OR its in-neighbours' masks (pull, early exit once
+// every missing bit is covered), then fix the newly seen bits, write their
+// levels and build the next active list.  A vertex reached by several
+// sources in the same round is expanded once for all of them, so 64 BFSs cost
+// a few passes over the graph instead of 64.  The direction switch uses the
+// single-source engine's rule (scout count against unexplored edges / alpha,
+// include/framework/hybrid_policy.h:265-288).  No reference counterpart: the
+// reference runs one source per Engine.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include <cmath>
+#include <cstddef>
+
+#include <type_traits>
+
+#include "sg_apps.cuh"
+#include "sg_bc.cuh"
+#include "sg_runtime.cuh"
+
+namespace {
+
+using namespace sepgraph;
+using engine::Ctrl;
+
+constexpr int kMsThreads = 256;
+constexpr uint32_t kMsBig = 256;  // vertices above this degree are expanded by a whole warp
+
+struct MsArgs {
+    const uint32_t *row, *col;    // CSR
+    const uint32_t *crow, *ccol;  // CSC (may alias CSR)
+    uint32_t nv, nsrc;
+    unsigned long long full;      // mask of the nsrc source bits
+    unsigned long long *seen, *fr[2], *next;
+    uint32_t *active[2], *touched;
+    const uint32_t *sources;
+    uint32_t *levels;  // nsrc rows of nv
+    Ctrl *ctrl;
+    uint32_t max_rounds;
+    double alpha;
+    long long total_edges;
+    unsigned long long timeout_ns;
+    int force_dir;  // -1 auto, 0 push, 1 pull
+};
+
+// Round snapshot in the control block's RoundState: variant = 0 push / 1 pull,
+// qin = active slot, F = active count, round, done.
+struct MsLeader {
+    long long unexplored;
+    uint32_t rounds_push, rounds_pull;
+};
+
+__device__ __forceinline__ uint32_t gthread() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint32_t nthreads() { return gridDim.x * blockDim.x; }
+
+__global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
+    Ctrl *c = a.ctrl;
+    engine::set_team(blockIdx.x, gridDim.x, c);
+    __shared__ engine::RoundState s;
+    engine::Counters *n = &c->cnt;
+    const uint32_t lane = dev::lane_id();
+    const uint32_t gw = gthread() >> 5, nw = nthreads() >> 5;
+    MsLeader L;
+    engine::PolicyState ps;  // leader's round state (block 0, thread 0)
+    auto nop = [] {};
+
+    // init: masks cleared, levels INF, sources seeded
+    for (uint32_t v = gthread(); v < a.nv; v += nthreads()) {
+        a.seen[v] = 0;
+        a.fr[0][v] = 0;
+        a.fr[1][v] = 0;
+        a.next[v] = 0;
+    }
+    const uint64_t total_lv = (uint64_t)a.nsrc * a.nv;
+    for (uint64_t k = gthread(); k < total_lv; k += nthreads()) a.levels[k] = 0xffffffffu;
+    if (!engine::grid_sync(c, a.timeout_ns, nop)) return;
+    if (gthread() < a.nsrc) {
+        const uint32_t v = a.sources[gthread()];
+        const unsigned long long bit = 1ull << gthread();
+        atomicOr(&a.seen[v], bit);
+        const unsigned long long old = atomicOr(&a.fr[0][v], bit);
+        if (old == 0) a.active[0][atomicAdd(&n->qcount[0], 1u)] = v;
+        a.levels[(uint64_t)gthread() * a.nv + v] = 0;
+    }
+    auto start = [&] {
+        memset(&ps, 0, sizeof ps);
+        ps.rs.round = 1;
+        ps.rs.qin = 0;
+        ps.rs.F = dev::ld_l2(&n->qcount[0]);
+        ps.rs.variant = a.force_dir == 1 ? 1 : 0;
+        L.unexplored = a.total_edges;
+        L.rounds_push = L.rounds_pull = 0;
+        const uint4 *src = reinterpret_cast<const uint4 *>(&ps.rs);
+        for (int k = 0; k < 4; ++k) __stcg(reinterpret_cast<uint4 *>(&c->rs) + k, src[k]);
+    };
+    if (!engine::grid_sync(c, a.timeout_ns, start)) return;
+
+    for (;;) {
+        if (threadIdx.x < 4)
+            reinterpret_cast<uint4 *>(&s)[threadIdx.x] = __ldcg(reinterpret_cast<const uint4 *>(&c->rs) + threadIdx.x);
+        __syncthreads();
+        if (s.done) break;
+        const uint32_t cur = s.qin, nxt = cur ^ 1u;
+        const unsigned long long *F = a.fr[cur];
+        unsigned long long edges = 0;
+        // ---- phase 1: expand
+        if (s.variant == 0) {
+            const uint32_t *act = a.active[cur];
+            for (uint32_t base = gw * 32; base < s.F; base += nw * 32) {
+                const uint32_t i = base + lane;
+                uint32_t v = 0, beg = 0, deg = 0;
+                unsigned long long f = 0;
+                if (i < s.F) {
+                    v = __ldcg(act + i);
+                    f = __ldcg(F + v);
+                    beg = __ldg(a.row + v);
+                    deg = __ldg(a.row + v + 1) - beg;
+                }
+                const bool big = deg > kMsBig;
+                if (!big) {
+                    for (uint32_t e = beg; e < beg + deg; ++e) {
+                        const uint32_t u = __ldg(a.col + e);
+                        const unsigned long long add = f & ~__ldcg(a.seen + u);
+                        if (add && (__ldcg(a.next + u) & add) != add) {
+                            const unsigned long long old = atomicOr(a.next + u, add);
+                            if (old == 0) a.touched[atomicAdd(&n->middle_count, 1u)] = u;
+                        }
+                    }
+                    edges += deg;
+                }
+                uint32_t m = __ballot_sync(dev::kFullMask, big);
+                while (m) {
+                    const uint32_t j = __ffs(m) - 1;
+                    m &= m - 1;
+                    const uint32_t bj = __shfl_sync(dev::kFullMask, beg, j), dj = __shfl_sync(dev::kFullMask, deg, j);
+                    const unsigned long long fj = __shfl_sync(dev::kFullMask, f, j);
+                    for (uint32_t k = lane; k < dj; k += 32) {
+                        const uint32_t u = __ldg(a.col + bj + k);
+                        const unsigned long long add = fj & ~__ldcg(a.seen + u);
+                        if (add && (__ldcg(a.next + u) & add) != add) {
+                            const unsigned long long old = atomicOr(a.next + u, add);
+                            if (old == 0) a.touched[atomicAdd(&n->middle_count, 1u)] = u;
+                        }
+                    }
+                    if (lane == 0) edges += dj;
+                }
+            }
+        } else {
+            // pull: every vertex that misses a source ORs its in-neighbours' frontier masks
+            for (uint32_t u = gthread(); u < a.nv; u += nthreads()) {
+                const unsigned long long miss = a.full & ~__ldcg(a.seen + u);
+                if (!miss) continue;
+                unsigned long long acc = 0;
+                const uint32_t b = __ldg(a.crow + u), e = __ldg(a.crow + u + 1);
+                uint32_t k = b;
+                for (; k < e; ++k) {
+                    acc |= __ldcg(F + __ldg(a.ccol + k));
+                    if ((acc & miss) == miss) {
+                        ++k;
+                        break;
+                    }
+                }
+                edges += k - b;
+                if (acc & miss) {
+                    a.next[u] = acc & miss;
+                    a.touched[atomicAdd(&n->middle_count, 1u)] = u;
+                }
+            }
+        }
+        edges = dev::warp_sum(edges);
+        if (lane == 0 && edges) atomicAdd(&n->edges_processed, edges);
+        if (!engine::grid_sync(c, a.timeout_ns, nop)) return;
+        // ---- phase 2: clear the old frontier, settle the new bits, build the next active list
+        {
+            const uint32_t *act = a.active[cur];
+            for (uint32_t i = gthread(); i < s.F; i += nthreads()) a.fr[cur][__ldcg(act + i)] = 0;
+            const uint32_t T = __ldcg(&n->middle_count);
+            unsigned long long scout = 0;
+            for (uint32_t base = gw * 32; base < T; base += nw * 32) {
+                const uint32_t i = base + lane;
+                uint32_t u = 0;
+                unsigned long long nb = 0;
+                if (i < T) {
+                    u = __ldcg(a.touched + i);
+                    nb = __ldcg(a.next + u) & ~__ldcg(a.seen + u);
+                    a.next[u] = 0;
+                    if (nb) {
+                        a.seen[u] |= nb;
+                        a.fr[nxt][u] = nb;
+                        scout += __ldg(a.row + u + 1) - __ldg(a.row + u);
+                        for (unsigned long long m = nb; m; m &= m - 1)
+                            a.levels[(uint64_t)(__ffsll(m) - 1) * a.nv + u] = s.round;
+                    }
+                }
+                dev::warp_append(a.active[nxt], &n->qcount[nxt], a.nv, nb != 0, u, &n->error);
+            }
+            scout = dev::warp_sum(scout);
+            if (lane == 0 && scout) atomicAdd(&n->scout[nxt], scout);
+        }
+        auto end_round = [&] {
+            const uint32_t F2 = dev::ld_l2(&n->qcount[nxt]);
+            const unsigned long long sc = dev::ld_l2(&n->scout[nxt]);
+            if (ps.rs.variant == 0) ++L.rounds_push; else ++L.rounds_pull;
+            L.unexplored -= (long long)sc;
+            if (L.unexplored < 0) L.unexplored = 0;
+            n->qcount[cur] = 0;
+            n->scout[cur] = 0;
+            n->middle_count = 0;
+            ps.rs.qin = nxt;
+            ps.rs.F = F2;
+            ps.rs.round++;
+            if (a.force_dir >= 0)
+                ps.rs.variant = a.force_dir;
+            else
+                ps.rs.variant = (double)sc > (double)L.unexplored / a.alpha ? 1 : 0;
+            if (F2 == 0 || ps.rs.round > a.max_rounds) {
+                ps.rs.done = 1;
+                c->round = ps.rs.round - 1;
+                c->rounds_by_variant[engine::V_ASYNC_PUSH_DD] = L.rounds_push;
+                c->rounds_by_variant[engine::V_ASYNC_PULL_DD] = L.rounds_pull;
+                c->max_iteration_reached = F2 != 0;
+            }
+            const uint4 *src = reinterpret_cast<const uint4 *>(&ps.rs);
+            for (int k = 0; k < 4; ++k) __stcg(reinterpret_cast<uint4 *>(&c->rs) + k, src[k]);
+        };
+        if (!engine::grid_sync(c, a.timeout_ns, end_round)) return;
+    }
+}
+
+// Edges of the reached component summed over sources: sum_v popcount(seen[v]) * deg(v).
+__global__ void msbfs_reach_kernel(const uint32_t *row, const unsigned long long *seen, uint32_t nv,
+                                   unsigned long long *out) {
+    unsigned long long e = 0;
+    for (uint32_t v = gthread(); v < nv; v += nthreads())
+        e += (unsigned long long)__popcll(seen[v]) * (__ldg(row + v + 1) - __ldg(row + v));
+    e = dev::warp_sum(e);
+    if ((threadIdx.x & 31) == 0 && e) atomicAdd(out, e);
+}
+
+}  // namespace
+
+extern "C" sg_status sg_msbfs(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt,
+                              uint32_t *levels_out, sg_stats *stats) {
+    if (!g || !g->ctx) return SG_ERR_INVALID_ARG;
+    return sgb::msbfs_on(g->ctx, g, sources, nsrc, opt, levels_out, stats);
+}
+
+extern "C" sg_status sg_msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint32_t nsrc,
+                                 const sg_options *opt, uint32_t *levels_out, sg_stats *stats) {
+    if (!ctx || !g || !g->ctx || g->ctx->device != ctx->device) return SG_ERR_INVALID_ARG;
+    return sgb::msbfs_on(ctx, g, sources, nsrc, opt, levels_out, stats);
+}
+
+// Multi-source BFS on any context of the graph's device; scratch comes from
+// that context, so concurrent calls on different contexts never share state.
+// With row_outs, row i goes to row_outs[i] (host or device, nv uint32 each)
+// and levels_out is ignored.
+sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt,
+                        uint32_t *levels_out, sg_stats *stats, uint32_t *const *row_outs) {
+    if (!ctx || !g || !sources || nsrc == 0 || nsrc > 64 || (!levels_out && !row_outs)) return SG_ERR_INVALID_ARG;
+    if (row_outs)
+        for (uint32_t i = 0; i < nsrc; ++i)
+            if (!row_outs[i]) return SG_ERR_INVALID_ARG;
+    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace;
+    for (uint32_t i = 0; i < nsrc; ++i)
+        if (sources[i] >= g->nv) return sgb::set_error(ctx, SG_ERR_INVALID_ARG, "source %u out of range", sources[i]);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ctx->device) cudaSetDevice(ctx->device);
+    struct Restore {
+        int p, d;
+        ~Restore() {
+            if (p >= 0 && p != d) cudaSetDevice(p);
+        }
+    } restore{prev, ctx->device};
+    sg_options o;
+    if (opt)
+        o = *opt;
+    else
+        sg_options_default(&o);
+    const uint32_t nv = g->nv;
+    auto &ws = *ctx->batch_ws;
+    MsArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.row = g->row;
+    a.col = g->col;
+    a.crow = g->has_csc ? g->crow : g->row;
+    a.ccol = g->has_csc ? g->ccol : g->col;
+    a.nv = nv;
+    a.nsrc = nsrc;
+    a.full = nsrc == 64 ? ~0ull : ((1ull << nsrc) - 1);
+    SG_TRY_CUDA(ctx, ws.get("ms_seen", nv, &a.seen));
+    SG_TRY_CUDA(ctx, ws.get("ms_fr0", nv, &a.fr[0]));
+    SG_TRY_CUDA(ctx, ws.get("ms_fr1", nv, &a.fr[1]));
+    SG_TRY_CUDA(ctx, ws.get("ms_next", nv, &a.next));
+    SG_TRY_CUDA(ctx, ws.get("q0", nv, &a.active[0]));
+    SG_TRY_CUDA(ctx, ws.get("q1", nv, &a.active[1]));
+    SG_TRY_CUDA(ctx, ws.get("middle", nv, &a.touched));
+    SG_TRY_CUDA(ctx, ws.get("ctrl", 1, &a.ctrl));
+    uint32_t *dsrc = nullptr;
+    SG_TRY_CUDA(ctx, ws.get("ms_sources", 64, &dsrc));
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(dsrc, sources, 4 * nsrc, cudaMemcpyHostToDevice, ctx->stream));
+    a.sources = dsrc;
+    const bool out_dev = !row_outs && sgb::is_device_ptr(levels_out, ctx->device);
+    if (out_dev)
+        a.levels = levels_out;
+    else
+        SG_TRY_CUDA(ctx, ws.get("ms_levels", (size_t)nsrc * nv, &a.levels));
+    a.max_rounds = o.max_iteration > 0 ? (uint32_t)o.max_iteration : 200u;
+    a.alpha = o.alpha > 0 ? o.alpha : 15;
+    a.total_edges = (long long)g->ne;
+    a.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
+    a.force_dir = o.variant == SG_ASYNC_PUSH_DD ? 0 : (o.variant == SG_ASYNC_PULL_DD ? 1 : -1);
+    if (!g->has_csc && !g->symmetric) a.force_dir = 0;
+
+    static int bps = 0;
+    if (!bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, msbfs_kernel, kMsThreads, 0));
+    const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : 4;
+    dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(bps, want)));
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    void *args[] = {&a};
+    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)msbfs_kernel, grid, dim3(kMsThreads), args, 0, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    if (!o.blocking) return SG_OK;
+    Ctrl h;
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(&h, a.ctrl, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    if (row_outs) {
+        for (uint32_t i = 0; i < nsrc; ++i)
+            SG_TRY_CUDA(ctx, cudaMemcpyAsync(row_outs[i], a.levels + (size_t)i * nv, 4ull * nv, cudaMemcpyDefault,
+                                             ctx->stream));
+    } else if (!out_dev) {
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync(levels_out, a.levels, 4ull * nsrc * nv, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    unsigned long long *dr = nullptr, reach = 0;
+    SG_TRY_CUDA(ctx, ws.get("reach_stats", 3, &dr));
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(dr, 0, 8, ctx->stream));
+    msbfs_reach_kernel<<<ctx->prop.multiProcessorCount * 4, 256, 0, ctx->stream>>>(g->row, a.seen, nv, dr);
+    SG_TRY_CUDA(ctx, cudaGetLastError());
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(&reach, dr, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    SG_TRY_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    const uint32_t bits = h.cnt.error;
+    if (stats) {
+        stats->rounds = h.round;
+        stats->max_iteration_reached = h.max_iteration_reached;
+        for (int k = 0; k < 8; ++k) stats->rounds_by_variant[k] = h.rounds_by_variant[k];
+        stats->time_total_ms = stats->time_kernel_ms = ms;
+        stats->edges_processed = h.cnt.edges_processed;
+        stats->edges_reached = reach;
+        stats->device_error = bits;
+    }
+    const sg_status st = sgb::device_error_status(bits);
+    if (st != SG_OK) return sgb::set_error(ctx, st, "msbfs device error bits 0x%x", bits);
+    return SG_OK;
+}
+
+// ---------------------------------------------------------------- many queries, one launch
+namespace {
+
+// Edges of the reached component of each query's value array (unreached = UINT32_MAX).
+__global__ void batch_reach_kernel(const uint32_t *const *rows, const uint32_t *const *vals, const uint32_t *nvs,
+                                   unsigned long long *out) {
+    const uint32_t q = blockIdx.y;
+    const uint32_t *row = rows[q], *val = vals[q];
+    const uint32_t nv = nvs[q];
+    unsigned long long e = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        if (val[v] != 0xffffffffu) e += __ldg(row + v + 1) - __ldg(row + v);
+    e = dev::warp_sum(e);
+    if ((threadIdx.x & 31) == 0 && e) atomicAdd(out + q, e);
+}
+
+// ---------------------------------------------------------------- batched BC
+// Per-team state of Brandes' two passes, sized for the largest graph.
+struct BCTeam {
+    uint32_t *level;  // forward levels (the engine's value array)
+    unsigned long long *sigma;
+    float *delta;
+    uint32_t *stack, *ends, *misc, *ccount;  // misc: 0 stack count, 1 levels closed, 2 search depth, 3 error bits
+    uint4 *chunks;
+    uint32_t chunk_cap, max_levels;
+};
+
+using BCApp = apps::BCForward<uint32_t, uint32_t, graphs::NoWeight>;
+
+// Each team claims a query, runs the hybrid forward pass (BCForward through the
+// same round loop as a single query) and then the backward pass over its own
+// level stack with team barriers, and writes delta * 0.5 to the query's
+// output.  Forward and backward of different queries overlap across teams.
+__global__ void __launch_bounds__(engine::kBlockThreads)
+    batched_bc_kernel(const engine::BatchQuery<BCApp, uint32_t> *queries, uint32_t nq,
+                      const engine::TeamSpace<uint32_t> *spaces, const BCTeam *bcs, float *const *outs,
+                      uint32_t team_blocks, uint32_t *next_query, engine::BatchResult *results, engine::Params p) {
+    using namespace engine;
+    const uint32_t team = blockIdx.x / team_blocks;
+    const TeamSpace<uint32_t> &sp = spaces[team];
+    const BCTeam bt = bcs[team];
+    Ctrl *c = sp.ctrl;
+    set_team(blockIdx.x % team_blocks, team_blocks, c);
+    const uint32_t gt = g_team_rank * blockDim.x + threadIdx.x, nt = g_team_size * blockDim.x;
+    __shared__ uint32_t s_q, s_misc[4];
+    auto nop = [] {};
+    for (;;) {
+        auto claim = [&] {
+            const uint32_t q = atomicAdd(next_query, 1u);
+            unsigned char *z = reinterpret_cast<unsigned char *>(&c->rs);
+            memset(z, 0, sizeof(Ctrl) - offsetof(Ctrl, rs));
+            c->pad0 = q;
+            for (int k = 0; k < 4; ++k) bt.misc[k] = 0;
+        };
+        if (!grid_sync(c, p.timeout_ns, claim)) return;
+        if (threadIdx.x == 0) s_q = dev::ld_l2(&c->pad0);
+        __syncthreads();
+        const uint32_t q = s_q;
+        if (q >= nq) return;
+        const BatchQuery<BCApp, uint32_t> &bq = queries[q];
+        const uint32_t nv = bq.csr.nnodes;
+        // sigma[source] = 1, every other path count and dependency 0 (hybrid_bc.cu:325-326);
+        // the engine's first team barrier orders these writes before the forward pass
+        for (uint32_t v = gt; v < nv; v += nt) {
+            bt.sigma[v] = v == bq.app.m_source_node ? 1ull : 0ull;
+            bt.delta[v] = 0.f;
+        }
+        for (uint32_t k = gt; k < bt.max_levels; k += nt) bt.ccount[k] = 0;
+        KArgs<uint32_t, uint32_t, graphs::NoWeight> a;
+        a.csr = bq.csr;
+        a.csc = bq.csc;
+        a.csr_w = bq.csr_w;
+        a.csc_w = bq.csc_w;
+        a.value = bt.level;
+        a.buffer = sp.buffer;
+        a.tmp = sp.tmp;
+        for (int k = 0; k < 3; ++k) {
+            a.queue[k] = sp.queue[k];
+            a.qflag[k] = sp.qflag[k];
+        }
+        a.bitmap[0] = sp.bitmap[0];
+        a.bitmap[1] = sp.bitmap[1];
+        a.queue_cap = nv;
+        a.nwords = nv / 32 + 1;
+        a.middle = sp.middle;
+        a.heavy = sp.heavy;
+        a.heavy_cap = sp.heavy_cap;
+        a.chunk_owner = sp.chunk_owner;
+        a.chunk_cap = sp.chunk_cap;
+        a.ctrl = c;
+        a.trace = nullptr;
+        a.trace_cap = 0;
+        a.p = p;
+        a.p.total_workload0 = (long long)bq.csr.nedges;
+        BCApp app = bq.app;
+        app.m_sigmas = bt.sigma;
+        app.m_p_search_depth = bt.misc + 2;
+        app.m_stack = apps::LevelStack{bt.stack, bt.misc + 0, bt.ends, bt.misc + 1, nv, bt.max_levels, bt.misc + 3};
+        app.m_p_current_round = &c->rs.round;
+        if (!run_instance<BCApp, uint32_t, uint32_t, graphs::NoWeight>(app, a)) return;
+        if (threadIdx.x < 4) s_misc[threadIdx.x] = dev::ld_l2(bt.misc + threadIdx.x);
+        __syncthreads();
+        const uint32_t nlevels = s_misc[1], depth = s_misc[2], ferr = s_misc[3];
+        // reached edges of the forward traversal (GTEPS numerator)
+        unsigned long long e = 0;
+        for (uint32_t v = gt; v < nv; v += nt)
+            if (__ldcg(bt.level + v) != 0xffffffffu) e += bq.csr.end_edge(v) - bq.csr.begin_edge(v);
+        e = dev::warp_sum(e);
+        if (dev::lane_id() == 0 && e) atomicAdd(&results[q].reached, e);
+        bc::BCBackArgs ba;
+        ba.row = bq.csr.row_start;
+        ba.col = bq.csr.edge_dst;
+        ba.level = bt.level;
+        ba.sigma = bt.sigma;
+        ba.delta = bt.delta;
+        ba.bc_out = outs[q];
+        ba.stack = bt.stack;
+        ba.ends = bt.ends;
+        ba.nlevels = nlevels;
+        ba.max_depth = (ferr == 0 && depth >= 2) ? min(depth - 1, nlevels ? nlevels - 1 : 0u) : 0u;
+        ba.nv = nv;
+        ba.chunks = bt.chunks;
+        ba.chunk_cap = bt.chunk_cap;
+        ba.chunk_count = bt.ccount;
+        ba.bar = nullptr;
+        ba.err = bt.misc + 3;
+        ba.timeout_ns = p.timeout_ns;
+        auto sync = [&] { return grid_sync(c, p.timeout_ns, nop); };
+        if (!bc::backward(ba, gt, nt, sync)) return;
+        // the result record follows every block's output writes
+        auto record = [&] { write_result(results + q, c, team, dev::ld_l2(bt.misc + 3), dev::globaltimer_ns()); };
+        if (!grid_sync(c, p.timeout_ns, record)) return;
+    }
+}
+
+template <typename T>
+sg_status ws_get(sg_ctx *ctx, const char *name, size_t n, T **out) {
+    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace;
+    SG_TRY_CUDA(ctx, ctx->batch_ws->get(name, n, out));
+    return SG_OK;
+}
+
+// Runs n queries of one functor type in one batched launch.  outs[i] receives
+// query i's value array (host or device memory of nv_i elements).
+template <typename App, typename TV, typename TB, typename TW>
+sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, const std::vector<sg_graph *> &graphs,
+                    const std::vector<void *> &outs, const sg_options &o, engine::Params p, sg_stats *stats,
+                    float *per_query_ms) {
+    using namespace engine;
+    const uint32_t n = (uint32_t)qs.size();
+    // largest graphs first (longest-processing-time order)
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return graphs[x]->ne > graphs[y]->ne; });
+    uint32_t nv_max = 0;
+    uint64_t ne_max = 0;
+    for (auto *g : graphs) {
+        nv_max = std::max(nv_max, g->nv);
+        ne_max = std::max(ne_max, g->ne);
+    }
+    constexpr bool kBC = std::is_same<App, BCApp>::value;
+    const void *kernel = kBC ? (const void *)batched_bc_kernel : (const void *)batched_engine_kernel<App, TV, TB, TW>;
+    static int max_bps = 0;
+    if (!max_bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_bps, kernel, kBlockThreads, 0));
+    const int bps = std::max(1, std::min(max_bps, o.blocks_per_sm > 0 ? o.blocks_per_sm : 4));
+    const uint32_t total_blocks = (uint32_t)(ctx->prop.multiProcessorCount * bps);
+    // Automatic team size: one block per 2M edges of the largest graph (64
+    // BFS/SSSP queries on RMAT scale 22 ran fastest with 37-74 blocks per team,
+    // 1.8x faster than one grid-wide team), and never fewer blocks than it
+    // takes to keep the whole grid busy when the batch has few queries.
+    uint32_t team_blocks = (uint32_t)o.reserved[0];
+    if (o.reserved[0] <= 0) {
+        team_blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ne_max >> 21, total_blocks));
+        team_blocks = std::max(team_blocks, total_blocks / n);
+    }
+    team_blocks = std::max(1u, std::min(team_blocks, total_blocks));
+    const uint32_t n_teams = std::max(1u, std::min(n, total_blocks / team_blocks));
+
+    // team workspaces
+    const uint32_t nwords = nv_max / 32 + 1;
+    const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(nv_max, ne_max / std::max(1u, p.heavy_threshold)) + 2;
+    const uint32_t chunk_cap = (uint32_t)(ne_max / p.chunk_edges + heavy_cap + 2);
+    TB *buf, *tmp;
+    uint32_t *qq, *bm, *fl, *mid, *chunk, *counter;
+    HeavyItem<TB> *heavy;
+    Ctrl *ctrl;
+    const size_t T = n_teams;
+    sg_status st;
+    if ((st = ws_get(ctx, "b_buf", T * nv_max * sizeof(TB) / sizeof(TB), &buf)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_tmp", T * nv_max, &tmp)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_q", T * 3 * nv_max, &qq)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_bm", T * 2 * nwords, &bm)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_fl", T * 3 * nwords, &fl)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_mid", T * nv_max, &mid)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_heavy", T * heavy_cap, &heavy)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_chunk", T * chunk_cap, &chunk)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_ctrl", T, &ctrl)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_counter", 1, &counter)) != SG_OK) return st;
+    // heavy/chunk tables start zeroed so that a stale chunk never names an out-of-range item
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(heavy, 0, T * heavy_cap * sizeof(HeavyItem<TB>), ctx->stream));
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(ctrl, 0, T * sizeof(Ctrl), ctx->stream));
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), ctx->stream));
+    std::vector<TeamSpace<TB>> spaces(T);
+    for (size_t t = 0; t < T; ++t) {
+        TeamSpace<TB> &s = spaces[t];
+        s.buffer = buf + t * nv_max;
+        s.tmp = tmp + t * nv_max;
+        for (int k = 0; k < 3; ++k) {
+            s.queue[k] = qq + (t * 3 + k) * nv_max;
+            s.qflag[k] = fl + (t * 3 + k) * nwords;
+        }
+        s.bitmap[0] = bm + (t * 2) * nwords;
+        s.bitmap[1] = bm + (t * 2 + 1) * nwords;
+        s.middle = mid + t * nv_max;
+        s.heavy = heavy + t * heavy_cap;
+        s.chunk_owner = chunk + t * chunk_cap;
+        s.ctrl = ctrl + t;
+        s.trace = nullptr;
+        s.cap_v = nv_max;
+        s.heavy_cap = heavy_cap;
+        s.chunk_cap = chunk_cap;
+        s.trace_cap = 0;
+    }
+    // BC: levels, path counts, dependencies, level stack and chunk table per team
+    BCTeam *dbc = nullptr;
+    float **douts = nullptr;
+    if constexpr (kBC) {
+        const uint32_t max_levels = std::min(p.max_iteration, nv_max) + 2;  // a level holds at least one vertex
+        const uint32_t bchunk_cap = (uint32_t)(ne_max / bc::kBcChunk + ne_max / bc::kBcBigDegree + 2);
+        uint32_t *lv, *stk, *ends, *misc, *cc;
+        unsigned long long *sig;
+        float *dl;
+        uint4 *bch;
+        if ((st = ws_get(ctx, "bc_level", T * nv_max, &lv)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "bc_sigma", T * nv_max, &sig)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "bc_delta", T * nv_max, &dl)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "bc_stack", T * nv_max, &stk)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "bc_ends", T * max_levels, &ends)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "bc_ccount", T * max_levels, &cc)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "bc_misc", T * 4, &misc)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "bc_chunks", T * bchunk_cap, &bch)) != SG_OK) return st;
+        std::vector<BCTeam> bts(T);
+        for (size_t t = 0; t < T; ++t)
+            bts[t] = BCTeam{lv + t * nv_max, sig + t * nv_max, dl + t * nv_max, stk + t * nv_max, ends + t * max_levels,
+                            misc + t * 4, cc + t * max_levels, bch + t * bchunk_cap, bchunk_cap, max_levels};
+        if ((st = ws_get(ctx, "bc_teams", T, &dbc)) != SG_OK) return st;
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync(dbc, bts.data(), T * sizeof(BCTeam), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    // outputs: device outputs are written in place, host outputs go through a staging array
+    std::vector<bool> out_dev(n);
+    TV *stage = nullptr;
+    size_t stage_elems = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        out_dev[i] = sgb::is_device_ptr(outs[i], ctx->device);
+        if (!out_dev[i]) stage_elems += graphs[i]->nv;
+    }
+    if (stage_elems && (st = ws_get(ctx, "b_stage", stage_elems, &stage)) != SG_OK) return st;
+    std::vector<TV *> vptr(n);
+    {
+        size_t off = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            vptr[i] = out_dev[i] ? (TV *)outs[i] : stage + off;
+            if (!out_dev[i]) off += graphs[i]->nv;
+        }
+    }
+    std::vector<BatchQuery<App, TV>> qd;
+    qd.reserve(n);
+    std::vector<float *> fouts(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        qd.push_back(qs[order[k]]);
+        qd.back().value = vptr[order[k]];
+        fouts[k] = reinterpret_cast<float *>(vptr[order[k]]);  // BC writes 4-byte floats in the same slots
+    }
+    if constexpr (kBC) {
+        if ((st = ws_get(ctx, "bc_outs", n, &douts)) != SG_OK) return st;
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync(douts, fouts.data(), n * sizeof(float *), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    BatchQuery<App, TV> *dq;
+    TeamSpace<TB> *dsp;
+    BatchResult *dres;
+    if ((st = ws_get(ctx, "b_queries", n, &dq)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_spaces", T, &dsp)) != SG_OK) return st;
+    if ((st = ws_get(ctx, "b_results", n, &dres)) != SG_OK) return st;
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(dq, qd.data(), n * sizeof(qd[0]), cudaMemcpyHostToDevice, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(dsp, spaces.data(), T * sizeof(spaces[0]), cudaMemcpyHostToDevice, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(dres, 0, n * sizeof(BatchResult), ctx->stream));
+    uint32_t tb = team_blocks;
+    void *args[] = {(void *)&dq, (void *)&n, (void *)&dsp, (void *)&tb, (void *)&counter, (void *)&dres, (void *)&p};
+    void *bc_args[] = {(void *)&dq,  (void *)&n,       (void *)&dsp,  (void *)&dbc, (void *)&douts,
+                       (void *)&tb,  (void *)&counter, (void *)&dres, (void *)&p};
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel(kernel, dim3(n_teams * team_blocks), dim3(kBlockThreads),
+                                                 kBC ? bc_args : args, 0, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    if (!o.blocking) return SG_OK;
+    std::vector<BatchResult> res(n);
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(res.data(), dres, n * sizeof(BatchResult), cudaMemcpyDeviceToHost, ctx->stream));
+    for (uint32_t i = 0; i < n; ++i)
+        if (!out_dev[i])
+            SG_TRY_CUDA(ctx, cudaMemcpyAsync(outs[i], vptr[i], graphs[i]->nv * sizeof(TV), cudaMemcpyDeviceToHost,
+                                             ctx->stream));
+    // reached edges per query (GTEPS numerator)
+    unsigned long long reached = 0;
+    if (stats && !kBC) {
+        const uint32_t **rows, **vals;
+        uint32_t *nvs;
+        unsigned long long *dr;
+        if ((st = ws_get(ctx, "b_rows", n, (const uint32_t ***)&rows)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "b_vals", n, (const uint32_t ***)&vals)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "b_nvs", n, &nvs)) != SG_OK) return st;
+        if ((st = ws_get(ctx, "b_reach", n, &dr)) != SG_OK) return st;
+        std::vector<const uint32_t *> hr(n), hv(n);
+        std::vector<uint32_t> hn(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            hr[i] = graphs[i]->row;
+            hv[i] = (const uint32_t *)vptr[i];
+            hn[i] = graphs[i]->nv;
+        }
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync(rows, hr.data(), n * sizeof(void *), cudaMemcpyHostToDevice, ctx->stream));
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync(vals, hv.data(), n * sizeof(void *), cudaMemcpyHostToDevice, ctx->stream));
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync(nvs, hn.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+        SG_TRY_CUDA(ctx, cudaMemsetAsync(dr, 0, n * sizeof(unsigned long long), ctx->stream));
+        if (sizeof(TV) == 4) {
+            batch_reach_kernel<<<dim3(64, n), 256, 0, ctx->stream>>>(rows, vals, nvs, dr);
+            SG_TRY_CUDA(ctx, cudaGetLastError());
+        }
+        std::vector<unsigned long long> hreach(n);
+        SG_TRY_CUDA(ctx, cudaMemcpyAsync(hreach.data(), dr, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        SG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        for (auto x : hreach) reached += x;
+    }
+    SG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    SG_TRY_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    uint32_t bits = 0;
+    std::vector<BatchResult> byq(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        byq[order[k]] = res[k];
+        bits |= res[k].error;
+        if (kBC) reached += 2 * res[k].reached;  // two traversals, as for a single BC query
+    }
+    if (stats) {
+        std::memset(stats->rounds_by_variant, 0, sizeof stats->rounds_by_variant);
+        stats->rounds = 0;
+        stats->edges_processed = 0;
+        stats->max_iteration_reached = 0;
+        for (auto &r : byq) {
+            stats->rounds = std::max(stats->rounds, r.rounds);
+            for (int k = 0; k < 8; ++k) stats->rounds_by_variant[k] += r.rounds_by_variant[k];
+            stats->edges_processed += r.edges_processed;
+            stats->max_iteration_reached |= r.max_iteration_reached;
+        }
+        stats->time_total_ms = stats->time_kernel_ms = ms;
+        stats->edges_reached = reached;
+        stats->vertices_processed = n;  // queries in the batch
+        stats->device_error = bits;
+        stats->search_depth = n_teams;  // teams used
+        stats->vertices_reached = team_blocks;
+    }
+    if (per_query_ms)
+        for (uint32_t i = 0; i < n; ++i) per_query_ms[i] = (float)((byq[i].t_end - byq[i].t_start) * 1e-6);
+    const sg_status dst = sgb::device_error_status(bits);
+    if (dst != SG_OK) return sgb::set_error(ctx, dst, "batch device error bits 0x%x", bits);
+    return SG_OK;
+}
+
+engine::Params batch_params(const sg_options &o, int scheme) {
+    engine::Params p;
+    std::memset(&p, 0, sizeof p);
+    p.scheme = scheme;
+    p.forced = o.variant;
+    if (o.alpha == 0) p.forced = engine::V_ASYNC_PUSH_DD;
+    p.lb_push = o.lb_push >= 0 ? o.lb_push : engine::LB_FINE;
+    p.lb_pull = o.lb_pull >= 0 ? o.lb_pull : engine::LB_FINE;
+    p.collect = p.forced < 0 ? 1 : 0;
+    p.has_csc = 1;
+    p.max_iteration = o.max_iteration > 0 ? (uint32_t)o.max_iteration : 200u;
+    p.heavy_threshold = o.heavy_degree > 0 ? (uint32_t)o.heavy_degree : 32u;
+    p.chunk_edges = o.chunk_edges > 0 ? (uint32_t)std::max(32, o.chunk_edges) : 256u;
+    p.pull_warp_threshold = 32;
+    p.alpha = o.alpha;
+    p.beta = o.beta > 0 ? o.beta : 18;
+    p.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
+    return p;
+}
+
+template <typename App>
+engine::BatchQuery<App, uint32_t> make_query(App app, sg_graph *g) {
+    engine::BatchQuery<App, uint32_t> bq{app, {}, {}, nullptr, nullptr, nullptr};
+    bq.csr.nnodes = g->nv;
+    bq.csr.nedges = (uint32_t)g->ne;
+    bq.csr.row_start = g->row;
+    bq.csr.edge_dst = g->col;
+    bq.csr.edge_weights = g->w;
+    bq.csc.nnodes = g->nv;
+    bq.csc.nedges = (uint32_t)g->ne;
+    bq.csc.col_start = g->crow ? g->crow : g->row;
+    bq.csc.edge_source = g->ccol ? g->ccol : g->col;
+    bq.csc.edge_weights = g->cw;
+    bq.csc.csr_row_start = g->row;
+    bq.csr_w = g->w;
+    bq.csc_w = g->cw;
+    bq.value = nullptr;
+    app.m_csr_graph = bq.csr;
+    app.m_csc_graph = bq.csc;
+    app.m_nnodes = g->nv;
+    app.m_nedges = (uint32_t)g->ne;
+    bq.app = app;
+    return bq;
+}
+
+sg_status check_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n) {
+    if (!ctx || !q || n == 0) return SG_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!q[i].graph || q[i].graph->ctx->device != ctx->device || !q[i].out)
+            return sgb::set_error(ctx, SG_ERR_INVALID_ARG, "query %u: graph on another device or null output", i);
+        if (q[i].source >= q[i].graph->nv)
+            return sgb::set_error(ctx, SG_ERR_INVALID_ARG, "query %u: source out of range", i);
+    }
+    return SG_OK;
+}
+
+struct DevGuard {
+    int prev = -1, dev;
+    explicit DevGuard(int d) : dev(d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevGuard() {
+        if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+extern "C" sg_status sg_sssp_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt,
+                                   sg_stats *stats, float *per_query_ms) {
+    sg_status st = check_batch(ctx, q, n);
+    if (st != SG_OK) return st;
+    DevGuard dg(ctx->device);
+    sg_options o;
+    if (opt)
+        o = *opt;
+    else
+        sg_options_default(&o);
+    engine::Params p = batch_params(o, 0);
+    using App = apps::SSSP<uint32_t, uint32_t, uint32_t>;
+    std::vector<engine::BatchQuery<App, uint32_t>> qs;
+    qs.reserve(n);
+    std::vector<sg_graph *> graphs(n);
+    std::vector<void *> outs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        App app(q[i].source);
+        qs.push_back(make_query(app, q[i].graph));
+        graphs[i] = q[i].graph;
+        outs[i] = q[i].out;
+        if (!q[i].graph->has_csc && p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
+    }
+    if (o.priority == SG_PRIORITY_LOW_HIGH) {
+        // one delta for the batch: the reference heuristic on the largest graph unless given
+        double delta = o.priority_delta;
+        if (delta <= 0) {
+            const sg_graph *g = *std::max_element(graphs.begin(), graphs.end(),
+                                                  [](const sg_graph *a, const sg_graph *b) { return a->ne < b->ne; });
+            delta = std::max(1.0, std::floor(32.0 * (g->ne ? g->weight_sum / g->ne : 1.0) / ((double)g->ne / g->nv)));
+        }
+        p.priority = 1;
+        p.prio_init_raw = p.prio_step_raw = engine::to_raw<uint32_t>((uint32_t)delta);
+        if (p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
+        p.collect = 0;
+    }
+    return run_batch<App, uint32_t, uint32_t, uint32_t>(ctx, qs, graphs, outs, o, p, stats, per_query_ms);
+}
+
+extern "C" sg_status sg_bfs_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt,
+                                  sg_stats *stats, float *per_query_ms) {
+    sg_status st = check_batch(ctx, q, n);
+    if (st != SG_OK) return st;
+    DevGuard dg(ctx->device);
+    sg_options o;
+    if (opt)
+        o = *opt;
+    else
+        sg_options_default(&o);
+    engine::Params p = batch_params(o, 0);
+    using App = apps::BFS<uint32_t, uint32_t, graphs::NoWeight>;
+    std::vector<engine::BatchQuery<App, uint32_t>> qs;
+    qs.reserve(n);
+    std::vector<sg_graph *> graphs(n);
+    std::vector<void *> outs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        App app(q[i].source, o.non_atomic != 0);
+        qs.push_back(make_query(app, q[i].graph));
+        graphs[i] = q[i].graph;
+        outs[i] = q[i].out;
+        if (!q[i].graph->has_csc && p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
+    }
+    return run_batch<App, uint32_t, uint32_t, graphs::NoWeight>(ctx, qs, graphs, outs, o, p, stats, per_query_ms);
+}
+
+extern "C" sg_status sg_bc_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt,
+                                 sg_stats *stats, float *per_query_ms) {
+    sg_status st = check_batch(ctx, q, n);
+    if (st != SG_OK) return st;
+    DevGuard dg(ctx->device);
+    sg_options o;
+    if (opt)
+        o = *opt;
+    else
+        sg_options_default(&o);
+    engine::Params p = batch_params(o, 0);
+    // HybridBC forces FINE_GRAINED load balancing (hybrid_bc.cu:335-336)
+    if (o.lb_push < 0) p.lb_push = engine::LB_FINE;
+    if (o.lb_pull < 0) p.lb_pull = engine::LB_FINE;
+    std::vector<engine::BatchQuery<BCApp, uint32_t>> qs;
+    qs.reserve(n);
+    std::vector<sg_graph *> graphs(n);
+    std::vector<void *> outs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        BCApp app(q[i].source, nullptr, nullptr, apps::LevelStack{});  // team state is bound on the device
+        qs.push_back(make_query(app, q[i].graph));
+        graphs[i] = q[i].graph;
+        outs[i] = q[i].out;
+        if (!q[i].graph->has_csc && p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
+    }
+    return run_batch<BCApp, uint32_t, uint32_t, graphs::NoWeight>(ctx, qs, graphs, outs, o, p, stats, per_query_ms);
+}

@@ -45,6 +45,15 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
 __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void st_relaxed(uint32_t *p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Barrier arrival: a release fence (this block's prior writes, ordered by the
+// preceding __syncthreads, become visible first) and a fire-and-forget add
+// whose result the arriving thread does not wait for.
+__device__ __forceinline__ void arrive_release(uint32_t *p) {
+    asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
+}
 // Loads of state that other blocks modify inside the same launch go through L2.
 template <typename T>
 __device__ __forceinline__ T ld_l2(const T *p) {

@@ -228,20 +228,44 @@ __device__ __forceinline__ int accumulate(App &app, const uint32_t *w, uint32_t 
 __device__ __forceinline__ bool acc_success(int st) { return st < 2; }
 __device__ __forceinline__ bool acc_continue(int st) { return st & 1; }
 
-// Bounded grid barrier with block 0 as the fixed leader.  Every other block
-// publishes its writes (fence) and arrives; block 0 waits for all arrivals,
-// runs `leader()` on one thread, and releases the generation.  A wait that
-// exceeds timeout_ns raises kErrTimeout (the leader still releases, so every
-// block leaves the kernel at its next status check) and returns false.
+// A team is the set of blocks that run one query together: the whole grid for
+// a single query, or one group of a batched launch.  Every block records its
+// rank in the team and the team size before the first barrier.
+__shared__ uint32_t g_team_rank, g_team_size;
+// Generation of the team barrier this block passed last (kept by thread 0).
+__shared__ uint32_t g_bar_gen;
+
+constexpr uint32_t kGenMask = 0x7fffffffu;   // generation counter bits
+constexpr uint32_t kGenAbort = 0x80000000u;  // set by a leader whose wait gave up
+
+// Joins the team and reads the barrier generation; must run before this
+// block's first arrival (no generation can pass without it).
+__device__ __forceinline__ void set_team(uint32_t rank, uint32_t size, Ctrl *c) {
+    if (threadIdx.x == 0) {
+        g_team_rank = rank;
+        g_team_size = size;
+        g_bar_gen = dev::ld_acquire(&c->bar_gen);
+    }
+    __syncthreads();
+}
+
+// Bounded team barrier with team rank 0 as the fixed leader.  Every other block
+// arrives with a release fence and a fire-and-forget add, then polls the
+// generation word; block 0 waits for all arrivals, runs `leader()` on one
+// thread and publishes the next generation with a release store.  Each block
+// tracks the generation it expects, so an arrival costs no read.  A wait that
+// exceeds timeout_ns raises kErrTimeout and returns false; a leader that gives
+// up releases the others with the abort bit set, so they return false too.
 template <typename Leader>
 __device__ __forceinline__ bool grid_sync(Ctrl *c, unsigned long long timeout_ns, Leader &&leader) {
     __shared__ uint32_t s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t ok = 1;
-        const uint32_t g = dev::ld_acquire(&c->bar_gen);
-        if (blockIdx.x == 0) {
-            const uint32_t need = gridDim.x - 1;
+        const uint32_t g = g_bar_gen;
+        uint32_t next = g;
+        if (g_team_rank == 0) {
+            const uint32_t need = g_team_size - 1;
             const uint64_t t0 = dev::globaltimer_ns();
             uint32_t spins = 0;
             while (dev::ld_acquire(&c->bar_count) < need) {
@@ -253,17 +277,17 @@ __device__ __forceinline__ bool grid_sync(Ctrl *c, unsigned long long timeout_ns
                 }
                 __nanosleep(20);
             }
-            __threadfence();
-            c->bar_count = 0;
+            dev::st_relaxed(&c->bar_count, 0u);  // ordered before the next arrivals by the release below
             if (ok) leader();
-            __threadfence();
-            dev::st_release(&c->bar_gen, g + 1);
+            next = ((g + 1) & kGenMask) | (ok ? 0u : kGenAbort);
+            dev::st_release(&c->bar_gen, next);
         } else {
-            __threadfence();
-            atomicAdd(&c->bar_count, 1u);
+            dev::arrive_release(&c->bar_count);
             const uint64_t t0 = dev::globaltimer_ns();
             uint32_t spins = 0;
-            while (dev::ld_acquire(&c->bar_gen) == g) {
+            for (;;) {
+                next = dev::ld_acquire(&c->bar_gen);
+                if (next != g) break;
                 ++spins;
                 if ((spins & 255u) == 0 && (dev::globaltimer_ns() - t0 > timeout_ns || spins > (1u << 28))) {
                     atomicOr(&c->cnt.error, dev::kErrTimeout);
@@ -272,9 +296,9 @@ __device__ __forceinline__ bool grid_sync(Ctrl *c, unsigned long long timeout_ns
                 }
                 __nanosleep(20);
             }
+            if (next & kGenAbort) ok = 0;
         }
-        __threadfence();
-        if (dev::ld_l2(&c->cnt.error) & dev::kErrTimeout) ok = 0;
+        g_bar_gen = next;
         s_ok = ok;
     }
     __syncthreads();
@@ -286,13 +310,21 @@ struct EngineKernel {
     using Args = KArgs<TV, TB, TW>;
     using Snap = RoundState;
 
-    static __device__ __forceinline__ uint32_t gthread() { return blockIdx.x * blockDim.x + threadIdx.x; }
-    static __device__ __forceinline__ uint32_t nthreads() { return gridDim.x * blockDim.x; }
+    static __device__ __forceinline__ uint32_t gthread() { return g_team_rank * blockDim.x + threadIdx.x; }
+    static __device__ __forceinline__ uint32_t nthreads() { return g_team_size * blockDim.x; }
     static __device__ __forceinline__ uint32_t gwarp() { return gthread() >> 5; }
     static __device__ __forceinline__ uint32_t nwarps() { return nthreads() >> 5; }
 
     static __device__ __forceinline__ uint32_t out_degree(const Args &a, uint32_t v) {
         return a.csr.end_edge(v) - a.csr.begin_edge(v);
+    }
+
+    // Out-degree of an appended vertex feeds the policy (scout count) and the
+    // heavy-vertex forecast; with a forced variant and no trace neither is
+    // needed and the two dependent loads are skipped (the round then always
+    // runs its chunk phase).
+    static __device__ __forceinline__ void count_enq(const Args &a, Acc &acc, bool hi, uint32_t v) {
+        if (a.p.collect) acc.count(hi, out_degree(a, v), a.p.heavy_threshold);
     }
 
     static __device__ void flush_acc(const Args &a, Acc &acc, uint32_t q_hi, uint32_t q_lo) {
@@ -328,7 +360,7 @@ struct EngineKernel {
         if (w_lo) w_lo = dev::bitmap_set(a.qflag[s.qlo], dst);
         dev::warp_append(a.queue[s.qhi], &n->qcount[s.qhi], a.queue_cap, w_hi, dst, &n->error);
         if (a.p.priority) dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, w_lo, dst, &n->error);
-        if (w_hi || w_lo) acc.count(w_hi, out_degree(a, dst), a.p.heavy_threshold);
+        if (w_hi || w_lo) count_enq(a, acc, w_hi, dst);
     }
 
     // Single-thread enqueue (LB NONE paths run divergent per-thread loops).
@@ -344,7 +376,7 @@ struct EngineKernel {
             a.queue[q][pos] = dst;
         else
             atomicOr(&n->error, dev::kErrCapacity);
-        acc.count(hi, out_degree(a, dst), a.p.heavy_threshold);
+        count_enq(a, acc, hi, dst);
     }
 
     // Registers the lanes' heavy vertices as chunk lists (warp-aggregated: one
@@ -408,21 +440,60 @@ struct EngineKernel {
         w.src[lane] = src;
         w.pay[lane] = payload;
         __syncwarp();
+        // Two-stage software pipeline: the next batch's owner lookup, index and
+        // weight loads (and an L2 prefetch of its destination state) are issued
+        // before the current batch's accumulate/enqueue chain.
+        EdgeRef cur = locate(a, w, lane, total);
         for (uint32_t eb = 0; eb < total; eb += 32) {
-            const uint32_t e = eb + lane;
+            const EdgeRef nxt = locate(a, w, eb + 32 + lane, total);
             bool want = false;
-            uint32_t dst = 0;
-            if (e < total) {
-                const uint32_t k = owner(w.excl, e);
-                const uint32_t edge = w.beg[k] + (e - w.excl[k]);
-                dst = a.csr.edge_dest(edge);
-                const int st = accumulate<App, TB, TW>(app, a.csr_w, w.src[k], dst, edge, a.buffer + dst, w.pay[k]);
+            if (cur.valid) {
+                const int st = accumulate_w(app, cur.src, cur.dst, cur.wt, a.buffer + cur.dst, cur.pay);
                 want = dd && acc_success(st);
             }
-            enqueue(app, a, s, dst, want, acc);
+            enqueue(app, a, s, cur.dst, want, acc);
+            cur = nxt;
         }
         if (lane == 0) acc.edges += total;
         __syncwarp();
+    }
+
+    struct EdgeRef {
+        uint32_t src, dst, wt;
+        TB pay;
+        bool valid;
+    };
+
+    // Edge e of the warp's concatenated edge lists: source, destination,
+    // weight (1 when unweighted) and payload; the destination's state line is
+    // prefetched into L2.
+    static __device__ __forceinline__ EdgeRef locate(const Args &a, const WarpLB<TB> &w, uint32_t e, uint32_t total) {
+        EdgeRef r;
+        r.valid = e < total;
+        r.src = 0;
+        r.dst = 0;
+        r.wt = 1;
+        r.pay = TB{};
+        if (r.valid) {
+            const uint32_t k = owner(w.excl, e);
+            const uint32_t edge = w.beg[k] + (e - w.excl[k]);
+            r.src = w.src[k];
+            r.pay = w.pay[k];
+            r.dst = a.csr.edge_dest(edge);
+            if constexpr (!std::is_same<TW, graphs::NoWeight>::value)
+                if (a.csr_w) r.wt = __ldg(a.csr_w + edge);
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(a.buffer + r.dst));
+        }
+        return r;
+    }
+
+    static __device__ __forceinline__ int accumulate_w(App &app, uint32_t src, uint32_t dst, uint32_t wt, TB *p,
+                                                       TB val) {
+        if constexpr (std::is_same<TW, graphs::NoWeight>::value) {
+            return app.App::AccumulateBuffer(src, dst, p, val);
+        } else {
+            return app.App::AccumulateBuffer(src, dst, (TW)wt, p, val);
+        }
     }
 
     // Thread-per-vertex sequential expansion honouring BREAK (LB NONE,
@@ -456,17 +527,30 @@ struct EngineKernel {
             const uint32_t off = (ch - h.chunk_base) * ce;
             if (off >= h.deg) continue;
             const uint32_t len = min(ce, h.deg - off);
-            for (uint32_t k = 0; k < len; k += 32) {
-                const uint32_t i = k + lane;
-                bool want = false;
-                uint32_t dst = 0;
+            auto load = [&](uint32_t i, uint32_t &dst, uint32_t &wt) {
+                dst = 0;
+                wt = 1;
                 if (i < len) {
                     const uint32_t edge = h.beg + off + i;
                     dst = a.csr.edge_dest(edge);
-                    const int st = accumulate<App, TB, TW>(app, a.csr_w, h.src, dst, edge, a.buffer + dst, h.payload);
+                    if constexpr (!std::is_same<TW, graphs::NoWeight>::value)
+                        if (a.csr_w) wt = __ldg(a.csr_w + edge);
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.buffer + dst));
+                }
+            };
+            uint32_t dst, wt;
+            load(lane, dst, wt);
+            for (uint32_t k = 0; k < len; k += 32) {
+                uint32_t ndst, nwt;
+                load(k + 32 + lane, ndst, nwt);
+                bool want = false;
+                if (k + lane < len) {
+                    const int st = accumulate_w(app, h.src, dst, wt, a.buffer + dst, h.payload);
                     want = dd && acc_success(st);
                 }
                 enqueue(app, a, s, dst, want, acc);
+                dst = ndst;
+                wt = nwt;
             }
             if (lane == 0) acc.edges += len;
         }
@@ -518,7 +602,7 @@ struct EngineKernel {
             }
             if (dd && s.pile) {
                 dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, keep, v, &n->error);
-                if (keep) acc.count(false, out_degree(a, v), a.p.heavy_threshold);
+                if (keep) count_enq(a, acc, false, v);
             }
             TB payload{};
             bool sched = false;
@@ -649,7 +733,7 @@ struct EngineKernel {
                     want = dev::bitmap_set(a.qflag[s.qhi], v);
                 }
                 dev::warp_append(a.queue[s.qhi], &n->qcount[s.qhi], a.queue_cap, want, v, &n->error);
-                if (want) acc.count(true, out_degree(a, v), a.p.heavy_threshold);
+                if (want) count_enq(a, acc, true, v);
             }
         }
     }
@@ -745,7 +829,7 @@ struct EngineKernel {
             if (v < N) act = app.App::IsActiveNode(v, dev::ld_l2(a.buffer + v));
             if (act) act = dev::bitmap_set(a.qflag[slot], v);
             dev::warp_append(a.queue[slot], &n->qcount[slot], a.queue_cap, act, v, &n->error);
-            if (act) acc.count(true, out_degree(a, v), a.p.heavy_threshold);
+            if (act) count_enq(a, acc, true, v);
         }
     }
 
@@ -805,7 +889,7 @@ struct EngineKernel {
         rs.bin = 0;
         rs.bout = 1;
         rs.F = min(dev::ld_l2(&n->qcount[0]), a.queue_cap);
-        rs.heavy_expected = dev::ld_l2(&n->heavy_enq[0]);
+        rs.heavy_expected = a.p.collect ? dev::ld_l2(&n->heavy_enq[0]) : (rs.F > 0);
         rs.prio_raw = a.p.prio_init_raw;
         ps.total_workload = a.p.total_workload0;
         pre_bookkeeping(a, ps, rs.F, dev::ld_l2(&n->scout[0]));
@@ -936,7 +1020,7 @@ struct EngineKernel {
         rs.variant = next;
         rs.round++;
         rs.F = min(qc[rs.qin], a.queue_cap);
-        rs.heavy_expected = he[rs.qin];
+        rs.heavy_expected = a.p.collect ? he[rs.qin] : (rs.F > 0);
         n->middle_count = 0;
         n->heavy_count = 0;
         n->chunk_count = 0;
@@ -960,8 +1044,10 @@ struct EngineKernel {
     }
 };
 
+// The whole round loop of one query, run by the calling team (set_team).
+// Returns false when a bounded wait gave up (the team must stop).
 template <typename App, typename TV, typename TB, typename TW>
-__global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App app_in, KArgs<TV, TB, TW> a) {
+__device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
     using K = EngineKernel<App, TV, TB, TW>;
     __shared__ RoundState s;
     __shared__ WarpLB<TB> wlb[kWarpsPerBlock];
@@ -987,10 +1073,10 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
         a.qflag[1][w] = 0;
         a.qflag[2][w] = 0;
     }
-    if (!grid_sync(c, tmo, nop)) return;
+    if (!grid_sync(c, tmo, nop)) return false;
     K::rebuild(app, a, 0, acc);
     K::flush_acc(a, acc, 0, 2);
-    if (!grid_sync(c, tmo, [&] { K::leader_start(a, ps); })) return;
+    if (!grid_sync(c, tmo, [&] { K::leader_start(a, ps); })) return false;
 
     WarpLB<TB> &my_lb = wlb[dev::warp_id()];
     const int lb_push = a.p.lb_push, lb_pull = a.p.lb_pull;
@@ -1005,7 +1091,7 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
                 K::push_phase_a(app, a, s, my_lb, true, lb_push, acc);
                 if (s.heavy_expected > 0 && lb_push != LB_NONE) {
                     K::flush_acc(a, acc, s.qhi, s.qlo);
-                    if (!grid_sync(c, tmo, nop)) return;
+                    if (!grid_sync(c, tmo, nop)) return false;
                     K::heavy_phase(app, a, s, true, acc);
                 }
                 K::flush_acc(a, acc, s.qhi, s.qlo);
@@ -1016,11 +1102,11 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
                 K::release_input_flags(a, s, false);
                 K::push_phase_a(app, a, s, my_lb, false, lb_push, acc);
                 K::flush_acc(a, acc, s.qhi, s.qlo);
-                if (!grid_sync(c, tmo, nop)) return;
+                if (!grid_sync(c, tmo, nop)) return false;
                 if (lb_push != LB_NONE) {
                     K::heavy_phase(app, a, s, false, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
-                    if (!grid_sync(c, tmo, nop)) return;
+                    if (!grid_sync(c, tmo, nop)) return false;
                 }
                 K::rebuild(app, a, s.qhi, acc);
                 K::flush_acc(a, acc, s.qhi, s.qlo);
@@ -1036,18 +1122,18 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
                 K::clear_dirty(a, s);
                 K::release_input_flags(a, s, convert);
                 K::combine_all(app, a, sync);
-                if (!grid_sync(c, tmo, nop)) return;
+                if (!grid_sync(c, tmo, nop)) return false;
                 if (reduce && !dd && lb_pull != LB_NONE) {
                     K::pull_reduce_td(app, a, s, my_lb, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
-                    if (!grid_sync(c, tmo, nop)) return;
+                    if (!grid_sync(c, tmo, nop)) return false;
                     K::pull_reduce_chunks(app, a, acc);
                 } else {
                     K::pull_phase(app, a, s, dd, sync, lb_pull, acc);
                 }
                 K::flush_acc(a, acc, s.qhi, s.qlo);
                 if (!dd) {
-                    if (!grid_sync(c, tmo, nop)) return;
+                    if (!grid_sync(c, tmo, nop)) return false;
                     K::rebuild(app, a, s.qhi, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                 }
@@ -1056,11 +1142,125 @@ __global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App 
             default:
                 break;  // unsupported variants never start a round (leader_start / leader_end_round)
         }
-        if (!grid_sync(c, tmo, [&] { K::leader_end_round(app, a, ps); })) return;
+        if (!grid_sync(c, tmo, [&] { K::leader_end_round(app, a, ps); })) return false;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (g_team_rank == 0 && threadIdx.x == 0) {
         c->edges_processed = dev::ld_l2(&c->cnt.edges_processed);
         c->error = dev::ld_l2(&c->cnt.error);
+    }
+    return true;
+}
+
+// One query: the whole cooperative grid is the team.
+template <typename App, typename TV, typename TB, typename TW>
+__global__ void __launch_bounds__(kBlockThreads) hybrid_engine_kernel(const App app_in, KArgs<TV, TB, TW> a) {
+    set_team(blockIdx.x, gridDim.x, a.ctrl);
+    run_instance<App, TV, TB, TW>(app_in, a);
+}
+
+// ---------------------------------------------------------------- batched queries
+// One query of a batch: its functor (source etc.), graph views and output.
+template <typename App, typename TV>
+struct BatchQuery {
+    App app;
+    graphs::dev::CSRGraph csr;
+    graphs::dev::CSCGraph csc;
+    const uint32_t *csr_w, *csc_w;
+    TV *value;
+};
+
+// Per-team workspace of a batched launch, sized for the largest graph of the
+// batch; every query a team runs reuses it.
+template <typename TB>
+struct TeamSpace {
+    TB *buffer, *tmp;
+    uint32_t *queue[3], *bitmap[2], *qflag[3], *middle, *chunk_owner;
+    HeavyItem<TB> *heavy;
+    Ctrl *ctrl;
+    sg_round_trace *trace;
+    uint32_t cap_v, heavy_cap, chunk_cap, trace_cap;
+};
+
+// Per-query result record written when the query finishes.
+struct BatchResult {
+    uint32_t rounds, error, max_iteration_reached, team;
+    uint32_t rounds_by_variant[8];
+    unsigned long long edges_processed, t_start, t_end;
+    unsigned long long reached;  // edges of the reached component, where the kernel counts it
+};
+
+// Leader-side record of a finished query (every field but `reached`).
+__device__ __forceinline__ void write_result(BatchResult *r, const Ctrl *c, uint32_t team, uint32_t extra_err,
+                                             unsigned long long t_end) {
+    r->rounds = c->round;
+    r->error = dev::ld_l2(&c->cnt.error) | extra_err;
+    r->max_iteration_reached = c->max_iteration_reached;
+    r->team = team;
+    for (int k = 0; k < 8; ++k) r->rounds_by_variant[k] = c->rounds_by_variant[k];
+    r->edges_processed = dev::ld_l2(&c->cnt.edges_processed);
+    r->t_start = c->t_start;
+    r->t_end = t_end;
+}
+
+// Batched engine: the cooperative grid is split into teams of team_blocks
+// blocks; each team takes the next query from a device counter (queries are
+// ordered largest first by the host), runs its whole round loop with a
+// team-local barrier, records its result and moves on.  Per-query frontiers
+// and state never leave the device; the batch is one launch (capturable in a
+// CUDA graph).
+template <typename App, typename TV, typename TB, typename TW>
+__global__ void __launch_bounds__(kBlockThreads)
+    batched_engine_kernel(const BatchQuery<App, TV> *queries, uint32_t nq, const TeamSpace<TB> *spaces,
+                          uint32_t team_blocks, uint32_t *next_query, BatchResult *results, Params p) {
+    const uint32_t team = blockIdx.x / team_blocks;
+    const TeamSpace<TB> &sp = spaces[team];
+    Ctrl *c = sp.ctrl;
+    set_team(blockIdx.x % team_blocks, team_blocks, c);
+    __shared__ uint32_t s_q;
+    for (;;) {
+        // the team leader claims the next query; zero its control state (barrier words excluded)
+        auto claim = [&] {
+            const uint32_t q = atomicAdd(next_query, 1u);
+            unsigned char *z = reinterpret_cast<unsigned char *>(&c->rs);
+            memset(z, 0, sizeof(Ctrl) - offsetof(Ctrl, rs));
+            c->pad0 = q;
+        };
+        if (!grid_sync(c, p.timeout_ns, claim)) return;
+        if (threadIdx.x == 0) s_q = dev::ld_l2(&c->pad0);
+        __syncthreads();
+        const uint32_t q = s_q;
+        if (q >= nq) return;
+        const BatchQuery<App, TV> &bq = queries[q];
+        KArgs<TV, TB, TW> a;
+        a.csr = bq.csr;
+        a.csc = bq.csc;
+        a.csr_w = bq.csr_w;
+        a.csc_w = bq.csc_w;
+        a.value = bq.value;
+        a.buffer = sp.buffer;
+        a.tmp = sp.tmp;
+        for (int k = 0; k < 3; ++k) {
+            a.queue[k] = sp.queue[k];
+            a.qflag[k] = sp.qflag[k];
+        }
+        a.bitmap[0] = sp.bitmap[0];
+        a.bitmap[1] = sp.bitmap[1];
+        a.queue_cap = bq.csr.nnodes;
+        a.nwords = bq.csr.nnodes / 32 + 1;
+        a.middle = sp.middle;
+        a.heavy = sp.heavy;
+        a.heavy_cap = sp.heavy_cap;
+        a.chunk_owner = sp.chunk_owner;
+        a.chunk_cap = sp.chunk_cap;
+        a.ctrl = c;
+        a.trace = nullptr;
+        a.trace_cap = 0;
+        a.p = p;
+        a.p.total_workload0 = (long long)bq.csr.nedges;
+        App app = bq.app;
+        app.m_p_current_round = &c->rs.round;
+        if (!run_instance<App, TV, TB, TW>(app, a)) return;
+        if (g_team_rank == 0 && threadIdx.x == 0) write_result(results + q, c, team, 0u, c->t_end);
     }
 }
 

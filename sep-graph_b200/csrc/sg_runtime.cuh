@@ -15,7 +15,12 @@
 #include <vector>
 
 #include "../../include/sepgraph.h"
+#include "sg_internal.h"
 #include "sg_engine.cuh"
+
+namespace sgb {
+struct Workspace;
+}
 
 struct sg_ctx {
     int device = 0;
@@ -29,6 +34,7 @@ struct sg_ctx {
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
     int live_graphs = 0;  // sg_destroy refuses while graphs of this context exist
+    sgb::Workspace *batch_ws = nullptr;  // scratch of batched launches (team workspaces)
 };
 
 namespace sgb {
@@ -301,6 +307,8 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     if (st != SG_OK) return set_error(ctx, st, "device error bits 0x%x", res->device_error());
     return SG_OK;
 }
+
+
 
 inline void fill_stats(sg_stats *s, const EngineResult &r) {
     if (!s) return;

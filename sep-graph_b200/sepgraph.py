@@ -80,6 +80,35 @@ class Stats(C.Structure):
         return d
 
 
+class BatchQuery(C.Structure):
+    _fields_ = [("graph", C.c_void_p), ("source", C.c_uint32), ("pad", C.c_uint32), ("out", C.c_void_p)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("max_batch", C.c_uint32),
+                ("max_pending", C.c_uint32), ("msbfs_min", C.c_uint32), ("sssp_delta", C.c_uint32),
+                ("pad", C.c_uint32), ("pr_error", C.c_double), ("reserved", C.c_int32 * 8)]
+
+
+class Query(C.Structure):
+    _fields_ = [("algo", C.c_int32), ("graph_id", C.c_uint32), ("source", C.c_uint32), ("pad", C.c_uint32),
+                ("out", C.c_void_p), ("out2", C.c_void_p)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("batches", C.c_uint64), ("pending", C.c_uint64), ("elapsed_s", C.c_double), ("qps", C.c_double),
+                ("mean_ms", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("p999_ms", C.c_double),
+                ("max_ms", C.c_double), ("hbm_budget", C.c_uint64), ("hbm_in_use", C.c_uint64),
+                ("hbm_peak", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+QUERY_ALGOS = {"bfs": 0, "sssp": 1, "pagerank": 2, "bc": 3}
+
+
 _lib = None
 _P = C.c_void_p
 _U32P = C.POINTER(C.c_uint32)
@@ -114,6 +143,23 @@ def load() -> C.CDLL:
         "sg_sssp": (C.c_int, [_P, C.c_uint32, C.POINTER(Options), _P, C.POINTER(Stats)]),
         "sg_pagerank": (C.c_int, [_P, C.POINTER(Options), _P, _P, C.POINTER(Stats)]),
         "sg_bc": (C.c_int, [_P, C.c_uint32, C.POINTER(Options), _P, _P, C.POINTER(Stats)]),
+        "sg_msbfs": (C.c_int, [_P, _U32P, C.c_uint32, C.POINTER(Options), _P, C.POINTER(Stats)]),
+        "sg_sssp_batch": (C.c_int, [_P, C.POINTER(BatchQuery), C.c_uint32, C.POINTER(Options), C.POINTER(Stats),
+                                    C.POINTER(C.c_float)]),
+        "sg_bfs_batch": (C.c_int, [_P, C.POINTER(BatchQuery), C.c_uint32, C.POINTER(Options), C.POINTER(Stats),
+                                   C.POINTER(C.c_float)]),
+        "sg_bc_batch": (C.c_int, [_P, C.POINTER(BatchQuery), C.c_uint32, C.POINTER(Options), C.POINTER(Stats),
+                                  C.POINTER(C.c_float)]),
+        "sg_msbfs_on": (C.c_int, [_P, _P, _U32P, C.c_uint32, C.POINTER(Options), _P, C.POINTER(Stats)]),
+        "sg_server_config_default": (C.c_int, [C.POINTER(ServerConfig)]),
+        "sg_server_create": (C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_P)]),
+        "sg_server_add_graph": (C.c_int, [_P, _P, _U32P]),
+        "sg_server_submit": (C.c_int, [_P, C.POINTER(Query), C.POINTER(C.c_uint64)]),
+        "sg_server_wait": (C.c_int, [_P, C.c_uint64, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+        "sg_server_drain": (C.c_int, [_P, C.c_double]),
+        "sg_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
+        "sg_server_reset_stats": (C.c_int, [_P]),
+        "sg_server_destroy": (C.c_int, [_P]),
         "sg_hgraph_gen_rmat": (C.c_int, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                          C.c_uint64, C.c_uint32, C.POINTER(_P)]),
         "sg_hgraph_gen_grid": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
@@ -319,6 +365,34 @@ class Context:
         _check(load().sg_device_info(self._c, C.byref(sm), C.byref(hbm), C.byref(l2), name, 256), "device_info")
         return {"sm_count": sm.value, "hbm_bytes": hbm.value, "l2_bytes": l2.value, "name": name.value.decode()}
 
+    def _batch(self, fn, name, queries, outs, team_blocks, opts, dtype=np.uint32):
+        n = len(queries)
+        arr = (BatchQuery * n)()
+        if outs is None:
+            outs = [np.empty(g.nv, dtype) for g, _ in queries]
+        for i, ((g, s), o) in enumerate(zip(queries, outs)):
+            arr[i].graph = g.handle
+            arr[i].source = int(s)
+            arr[i].out = _ptr(o)
+        o = make_options(**opts)
+        if team_blocks:
+            o.reserved[0] = int(team_blocks)
+        st = Stats()
+        per = (C.c_float * n)()
+        _check(fn(self._c, arr, n, C.byref(o), C.byref(st), per), name, self._c)
+        return outs, st, list(per)
+
+    def sssp_batch(self, queries, outs=None, team_blocks: int = 0, **opts):
+        """queries: list of (Graph, source).  One launch; returns (outputs, stats, per-query ms)."""
+        return self._batch(load().sg_sssp_batch, "sg_sssp_batch", queries, outs, team_blocks, opts)
+
+    def bfs_batch(self, queries, outs=None, team_blocks: int = 0, **opts):
+        return self._batch(load().sg_bfs_batch, "sg_bfs_batch", queries, outs, team_blocks, opts)
+
+    def bc_batch(self, queries, outs=None, team_blocks: int = 0, **opts):
+        """Single-source BC of every (Graph, source) in one launch; outputs are float32 arrays."""
+        return self._batch(load().sg_bc_batch, "sg_bc_batch", queries, outs, team_blocks, opts, np.float32)
+
     def graph(self, hg: HostGraph, symmetric: bool = False, no_csc: bool = False) -> "Graph":
         g = _P()
         flags = (GRAPH_SYMMETRIC if symmetric else 0) | (GRAPH_NO_CSC if no_csc else 0)
@@ -345,6 +419,59 @@ class Context:
                 g.close()
             load().sg_destroy(self._c)
             self._c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching query server (sg_server_*)."""
+
+    def __init__(self, device: int = 0, **cfg):
+        c = ServerConfig()
+        _check(load().sg_server_config_default(C.byref(c)), "server_config_default")
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        self._s = _P()
+        _check(load().sg_server_create(device, C.byref(c), C.byref(self._s)), "sg_server_create")
+        self._keep = {}
+
+    def add_graph(self, g: "Graph") -> int:
+        gid = C.c_uint32()
+        _check(load().sg_server_add_graph(self._s, g.handle, C.byref(gid)), "sg_server_add_graph")
+        return gid.value
+
+    def submit(self, algo: str, graph_id: int, source: int, out, out2=None) -> int:
+        q = Query(QUERY_ALGOS[algo], graph_id, source, 0, _ptr(out), _ptr(out2))
+        t = C.c_uint64()
+        _check(load().sg_server_submit(self._s, C.byref(q), C.byref(t)), "sg_server_submit")
+        self._keep[t.value] = (out, out2)  # host buffers must outlive the query
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = 600.0):
+        st, lat = C.c_int(), C.c_double()
+        _check(load().sg_server_wait(self._s, ticket, timeout_s, C.byref(st), C.byref(lat)), "sg_server_wait")
+        self._keep.pop(ticket, None)
+        return st.value, lat.value
+
+    def drain(self, timeout_s: float = 600.0):
+        _check(load().sg_server_drain(self._s, timeout_s), "sg_server_drain")
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(load().sg_server_get_stats(self._s, C.byref(s)), "sg_server_get_stats")
+        return s.as_dict()
+
+    def reset_stats(self):
+        _check(load().sg_server_reset_stats(self._s), "sg_server_reset_stats")
+
+    def close(self):
+        if self._s:
+            load().sg_server_destroy(self._s)
+            self._s = None
 
     def __del__(self):
         try:
@@ -413,6 +540,17 @@ class Graph:
         _check(load().sg_pagerank(self._g, C.byref(o), _ptr(out), _ptr(residual_out), C.byref(st)), "sg_pagerank",
                self.ctx.handle)
         return out, st, self._trace(buf, st)
+
+    def msbfs(self, sources, out=None, **opts):
+        """BFS from up to 64 sources in one launch; returns (levels[nsrc, nv], stats)."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        o = make_options(**opts)
+        if out is None:
+            out = np.empty((len(src), self.nv), np.uint32)
+        st = Stats()
+        _check(load().sg_msbfs(self._g, src.ctypes.data_as(_U32P), len(src), C.byref(o), _ptr(out), C.byref(st)),
+               "sg_msbfs", self.ctx.handle)
+        return out, st
 
     def bc(self, source: int, out=None, sigma_out=None, trace_capacity: int = 0, **opts):
         o = make_options(**opts)

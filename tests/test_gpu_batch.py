@@ -1,0 +1,137 @@
+"""Batched execution parity: every row of a multi-source BFS equals the
+single-source oracle BFS from that source, bit for bit, whatever the batch
+size, direction policy, duplicates or graph shape."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import sepgraph as sg
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = sg.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_msbfs_golden(ctx, path):
+    z = np.load(path)
+    off, idx = z["offsets"], z["indices"]
+    nv = len(off) - 1
+    G = ctx.graph_from_csr(off, idx)
+    srcs = np.arange(min(nv, 64), dtype=np.uint32)
+    for variant in ("auto", "async_push_dd", "async_pull_dd"):
+        lv, st = G.msbfs(srcs, variant=variant)
+        for i, s in enumerate(srcs):
+            assert (lv[i] == oracle.bfs(off, idx, int(s))).all(), (variant, s)
+
+
+@pytest.mark.parametrize("scale,sym,n", [(14, True, 64), (15, False, 33), (16, True, 1), (16, True, 64)])
+def test_msbfs_rmat(ctx, scale, sym, n):
+    h = sg.HostGraph.rmat(scale, 16, symmetric=sym, seed=2)
+    G = ctx.graph(h, symmetric=sym)
+    srcs = h.pick_sources(n, 5)
+    srcs[-1] = srcs[0]  # a duplicate source
+    for variant in ("auto", "async_push_dd", "async_pull_dd"):
+        lv, st = G.msbfs(srcs, variant=variant)
+        for i in range(n):
+            assert (lv[i] == oracle.bfs(h.offsets, h.indices, int(srcs[i]))).all(), (variant, i)
+    deg = np.diff(h.offsets.astype(np.int64))
+    reached = sum(int(deg[row != sg.INF].sum()) for row in lv)
+    assert st.edges_reached == reached
+
+
+def test_msbfs_matches_single_source_engine(ctx):
+    h = sg.HostGraph.grid(64, 80)
+    G = ctx.graph(h)
+    srcs = np.array([0, 5119, 2500, 77], np.uint32)
+    lv, st = G.msbfs(srcs, max_iteration=100000)
+    for i, s in enumerate(srcs):
+        single, _, _ = G.bfs(int(s), max_iteration=100000)
+        assert (lv[i] == single).all()
+
+
+@pytest.fixture(scope="module")
+def uneven_graphs(ctx):
+    """Graphs of uneven size (RMAT scales 8-14, directed and symmetric, a grid), weights in [1,64)."""
+    out = []
+    for k, (scale, sym) in enumerate([(8, False), (10, True), (12, False), (13, True), (14, False), (11, False)]):
+        h = sg.HostGraph.rmat(scale, 16, symmetric=sym, seed=10 + k).gen_weights(1, 64, 3 + k)
+        out.append((h, ctx.graph(h, symmetric=sym)))
+    h = sg.HostGraph.grid(40, 50).gen_weights(1, 64, 99)
+    out.append((h, ctx.graph(h)))
+    return out
+
+
+@pytest.mark.parametrize("team_blocks", [0, 1, 8])
+def test_sssp_batch_uneven_graphs(ctx, uneven_graphs, team_blocks):
+    queries, refs = [], []
+    for k in range(40):
+        h, G = uneven_graphs[k % len(uneven_graphs)]
+        s = int(h.pick_sources(1, 100 + k)[0])
+        queries.append((G, s))
+        refs.append(oracle.sssp(h.offsets, h.indices, h.weights, s))
+    for kw in (dict(max_iteration=100000), dict(priority="low_high", max_iteration=1000000),
+               dict(variant="async_push_dd", max_iteration=100000)):
+        outs, st, per = ctx.sssp_batch(queries, team_blocks=team_blocks, **kw)
+        for i, (o, r) in enumerate(zip(outs, refs)):
+            assert (o == r).all(), (kw, i)
+        assert st.edges_reached == sum(int(np.diff(h.offsets.astype(np.int64))[r != sg.INF].sum())
+                                       for (h, _), r in zip([uneven_graphs[k % len(uneven_graphs)] for k in range(40)],
+                                                            refs))
+        assert all(p >= 0 for p in per)
+
+
+def test_bfs_batch_matches_single(ctx, uneven_graphs):
+    queries = [(G, int(h.pick_sources(1, k)[0])) for k, (h, G) in enumerate(uneven_graphs)] * 3
+    torch = pytest.importorskip("torch")
+    outs = [torch.empty(G.nv, dtype=torch.int32, device="cuda") for G, _ in queries]  # device outputs
+    outs, st, _ = ctx.bfs_batch(queries, outs=outs)
+    ctx.synchronize()
+    for (G, s), o in zip(queries, outs):
+        single, _, _ = G.bfs(s)
+        assert (o.cpu().numpy().view(np.uint32) == single).all()
+
+
+def test_msbfs_rejects_bad_batches(ctx):
+    h = sg.HostGraph.rmat(10, 8, seed=1)
+    G = ctx.graph(h)
+    with pytest.raises(sg.SGError):
+        G.msbfs(np.arange(65, dtype=np.uint32))
+    with pytest.raises(sg.SGError):
+        G.msbfs(np.array([h.nv], np.uint32))
+
+
+@pytest.mark.parametrize("team_blocks", [0, 2])
+def test_bc_batch_matches_single_and_oracle(ctx, team_blocks):
+    """Batched BC over uneven graphs (unweighted view): each output equals sg_bc
+    from that source within 1e-4 relative, and the FP64 oracle on small graphs."""
+    specs = [("rmat", 9, True, 1), ("rmat", 11, True, 2), ("grid", (20, 30), False, 3), ("rmat", 12, False, 4)]
+    graphs = []
+    for kind, p, sym, seed in specs:
+        h = sg.HostGraph.rmat(p, 8, symmetric=sym, seed=seed) if kind == "rmat" else sg.HostGraph.grid(*p)
+        graphs.append((h, ctx.graph(h, symmetric=sym)))
+    queries, hosts = [], []
+    for k in range(18):
+        h, G = graphs[k % len(graphs)]
+        queries.append((G, int(h.pick_sources(1, 50 + k)[0])))
+        hosts.append(h)
+    queries.append((graphs[0][1], queries[0][1]))  # the same query twice in one batch
+    hosts.append(graphs[0][0])
+    outs, st, per = ctx.bc_batch(queries, team_blocks=team_blocks, max_iteration=100000)
+    assert st.device_error == 0 and all(p >= 0 for p in per)
+    for (G, s), h, o in zip(queries, hosts, outs):
+        single, _, _ = G.bc(s, max_iteration=100000)
+        assert np.allclose(o, single, rtol=1e-4, atol=1e-5), s
+        if h.nv <= 1024:
+            want, _, _ = oracle.bc_f64(h.offsets, h.indices, s)
+            assert np.allclose(o, want, rtol=1e-4, atol=1e-4), s

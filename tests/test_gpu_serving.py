@@ -1,0 +1,140 @@
+"""Serving: a mixed BFS/SSSP/PageRank/BC stream submitted while earlier
+batches run; every result must equal the same query run alone through the
+single-query API (bit-exact for BFS/SSSP, PageRank L1 <= 1e-6 of normalised
+vectors, BC within 1e-4 relative)."""
+import random
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import sepgraph as sg
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    ctx = sg.Context(0)
+    specs = [("rmat", 10, True), ("rmat", 12, False), ("grid", (30, 40), False), ("rmat", 13, True)]
+    graphs = []
+    for k, (kind, p, sym) in enumerate(specs):
+        h = sg.HostGraph.rmat(p, 16, symmetric=sym, seed=20 + k) if kind == "rmat" else sg.HostGraph.grid(*p)
+        h.gen_weights(1, 64, 30 + k)
+        graphs.append((h, ctx.graph(h, symmetric=sym)))
+    yield ctx, graphs
+    ctx.close()
+
+
+def _pr_l1(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.abs(a / a.sum() - b / b.sum()).sum()
+
+
+def _mixed(graphs, n, seed):
+    rng = random.Random(seed)
+    qs = []
+    for _ in range(n):
+        r = rng.random()
+        algo = "bfs" if r < 0.60 else "sssp" if r < 0.85 else "pagerank" if r < 0.95 else "bc"
+        gid = rng.randrange(len(graphs))
+        h = graphs[gid][0]
+        src = int(h.pick_sources(1, rng.randrange(1 << 30))[0])
+        qs.append((algo, gid, src))
+    return qs
+
+
+def _alone(graphs, algo, gid, src):
+    G = graphs[gid][1]
+    if algo == "bfs":
+        return G.bfs(src)[0]
+    if algo == "sssp":
+        return G.sssp(src, variant="async_push_dd", max_iteration=1000000)[0]
+    if algo == "pagerank":
+        return G.pagerank(pr_error=1e-7, max_iteration=100000)[0]
+    return G.bc(src)[0]
+
+
+def _check(graphs, algo, gid, src, got):
+    want = _alone(graphs, algo, gid, src)
+    if algo in ("bfs", "sssp"):
+        assert (got == want).all(), (algo, gid, src)
+    elif algo == "pagerank":
+        assert _pr_l1(got, want) <= 1e-6
+    else:
+        assert np.allclose(got, want, rtol=1e-4, atol=1e-5)
+
+
+def test_results_same_alone_and_in_the_mix(setup):
+    ctx, graphs = setup
+    srv = sg.Server(0, slots=3, max_batch=64)
+    try:
+        gids = [srv.add_graph(G) for _, G in graphs]
+        assert gids == list(range(len(graphs)))
+        queries = _mixed(graphs, 240, seed=7)
+        outs = [np.zeros(graphs[g][0].nv, np.float32 if a in ("pagerank", "bc") else np.uint32)
+                for a, g, _ in queries]
+        tickets = [None] * len(queries)
+        errors = []
+
+        def producer():  # arrivals keep coming while earlier batches are on the GPU
+            rng = random.Random(3)
+            try:
+                for i, (a, g, s) in enumerate(queries):
+                    tickets[i] = srv.submit(a, g, s, outs[i])
+                    if rng.random() < 0.2:
+                        time.sleep(rng.expovariate(2000.0))
+            except Exception as e:  # reported by the main thread
+                errors.append(repr(e))
+
+        th = threading.Thread(target=producer)
+        th.start()
+        th.join()
+        assert not errors, errors
+        statuses = [srv.wait(t) for t in tickets]
+        bad = [(q, st) for q, st in zip(queries, statuses) if st[0] != 0 or st[1] < 0]
+        assert not bad, bad[:5]
+        st = srv.stats()
+        assert st["completed"] == len(queries) and st["failed"] == 0, st
+        assert st["batches"] < len(queries), "queries were batched"
+        assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"], st
+        assert st["hbm_peak"] <= st["hbm_budget"], st
+    finally:
+        srv.close()  # waits for the workers before the graphs go away
+    for (a, g, s), o in zip(queries, outs):
+        _check(graphs, a, g, s, o)
+
+
+def test_tiny_budget_still_serves_one_at_a_time(setup):
+    ctx, graphs = setup
+    srv = sg.Server(0, slots=2, max_batch=32, hbm_budget_bytes=1)
+    try:
+        for _, G in graphs:
+            srv.add_graph(G)
+        queries = _mixed(graphs, 30, seed=11)
+        outs = [np.zeros(graphs[g][0].nv, np.float32 if a in ("pagerank", "bc") else np.uint32)
+                for a, g, _ in queries]
+        ts = [srv.submit(a, g, s, o) for (a, g, s), o in zip(queries, outs)]
+        statuses = [srv.wait(t)[0] for t in ts]
+        assert statuses == [0] * len(ts), statuses
+        st = srv.stats()
+        assert st["completed"] == len(queries) and st["batches"] >= len(queries) // 2, st
+    finally:
+        srv.close()
+    for (a, g, s), o in zip(queries, outs):
+        _check(graphs, a, g, s, o)
+
+
+def test_submit_validation(setup):
+    ctx, graphs = setup
+    srv = sg.Server(0, slots=1)
+    try:
+        srv.add_graph(graphs[0][1])
+        out = np.zeros(graphs[0][0].nv, np.uint32)
+        with pytest.raises(sg.SGError):
+            srv.submit("bfs", 5, 0, out)  # unknown graph
+        with pytest.raises(sg.SGError):
+            srv.submit("bfs", 0, graphs[0][0].nv, out)  # source out of range
+    finally:
+        srv.close()
