@@ -1,18 +1,32 @@
 #!/usr/bin/env python
-"""Benchmark: single-source SSSP on RMAT scale 22 (edge factor 16, a/b/c/d =
-.57/.19/.19/.05, seed 1, directed, uint32 weights uniform in [1,64) seed 2),
-eight seeded sources (seed 3) per step, through the library's C ABI.
+"""Benchmark of the B200 hybrid graph engine through its C ABI.
 
-Metric: GTEPS = edges in the reached component / solve time, summed over the
-step's sources and over ranks (replicas, one process per GPU, weak scaling).
+Headline (one JSON line): single-source SSSP on RMAT scale 22 (edge factor 16,
+a/b/c/d = .57/.19/.19/.05, seed 1, directed, uint32 weights uniform in [1,64)
+seed 2), eight seeded sources (seed 3) per step.  GTEPS = edges of the reached
+component / solve time, summed over the step's sources and over ranks
+(replicas, one process per GPU, weak scaling).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--all]
+At N=1 the line also carries, under "extra" (skip with --quick):
+  per_algo  BFS RMAT-16 symmetric (the reference's host-checker case, its
+            BFSHost timed beside), SSSP on the 4096x4096 grid (weights
+            [1,1000), delta autotuned), PageRank on RMAT-23 directed
+            (data-driven push and topology-driven pull, residual 1e-7), BC on
+            RMAT-23 symmetrised — GTEPS and fraction of the HBM roofline each;
+  batched   64-source BFS and 32-source BC on RMAT-22 symmetric, 256 SSSP
+            instances over RMAT scale 12-20 graphs: one launch vs one plain
+            launch per query, results compared;
+  served    a Poisson stream of mixed BFS/SSSP/PageRank/BC queries
+            (60/25/10/5 %) over 16 device-resident graphs (RMAT 14-22, grids
+            1024^2-4096^2) through the query server: queries/s and
+            p50/p99/p999 latency, against the plain one-query-per-launch path
+            timed on a uniform sample of the same stream, results compared.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--quick]
 
 --impl reference times the reference's own single-threaded SSSPHostNaive
 (compiled from its sources into oracle/_ref; the oracle's C port otherwise)
 on the host cores, one source per thread, on the same graph and sources.
---all adds the other configurations (BFS RMAT-16, PageRank RMAT-23, BC
-RMAT-23 symmetrised, SSSP on the 4096x4096 grid) as extra keys.
 """
 from __future__ import annotations
 
@@ -21,9 +35,11 @@ import concurrent.futures as cf
 import datetime
 import json
 import os
+import random
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -36,6 +52,7 @@ METRIC = "GTEPS"
 WORKLOAD = "sssp_rmat22_directed_w1-64"
 SCALE, EDGE_FACTOR, N_SOURCES = 22, 16, 8
 FALLBACK_HBM_GBS = 6650.0
+INF = 0xFFFFFFFF
 
 
 def args_parse():
@@ -44,7 +61,8 @@ def args_parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--all", action="store_true")
+    p.add_argument("--quick", action="store_true", help="headline line only")
+    p.add_argument("--served-queries", type=int, default=1000)
     p.add_argument("--scale", type=int, default=SCALE)
     p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc"],
                    help="run one warm-up and one measured solve of that kernel only (for ncu captures)")
@@ -66,7 +84,7 @@ def run_profile(a):
         if a.profile == "sssp_push":
             _, st, _ = G.sssp(src, variant="async_push_dd", max_iteration=100000)
         elif a.profile == "sssp_delta":
-            _, st, _ = G.sssp(src, priority="low_high", max_iteration=1000000)
+            _, st, _ = G.sssp(src, priority="low_high", priority_delta=8, max_iteration=1000000)
         elif a.profile == "bfs":
             _, st, _ = G.bfs(src)
         elif a.profile == "pr_pull":
@@ -144,6 +162,16 @@ def sssp_bytes(nv, e_reached):
     return 4 * (nv + 1) + 8 * e_reached + 4 * nv
 
 
+def bfs_bytes(nv, e_reached):
+    # offsets + index per reached edge + levels
+    return 4 * (nv + 1) + 4 * e_reached + 4 * nv
+
+
+def reached_edges(h, values):
+    deg = np.diff(h.offsets.astype(np.int64))
+    return int(deg[np.asarray(values) != INF].sum())
+
+
 # ---------------------------------------------------------------- reference arm / CPU baseline
 def cpu_sssp_one(h, src):
     import oracle
@@ -155,14 +183,13 @@ def cpu_sssp_one(h, src):
 
 def cpu_baseline(h, srcs, budget_s=20.0):
     """Single thread, as many sources as fit the budget (>= 1)."""
-    deg = np.diff(h.offsets.astype(np.int64))
     t_tot, e_tot, n = 0.0, 0, 0
     kind = "port"
     for s in srcs:
         t0 = time.perf_counter()
         d, kind = cpu_sssp_one(h, s)
         t_tot += time.perf_counter() - t0
-        e_tot += int(deg[d != 0xFFFFFFFF].sum())
+        e_tot += reached_edges(h, d)
         n += 1
         if t_tot > budget_s:
             break
@@ -176,7 +203,6 @@ def run_reference(a):
     if rank != 0:
         return
     h, srcs = make_graph(a.scale)
-    deg = np.diff(h.offsets.astype(np.int64))
     ncores = os.cpu_count() or 1
     nthreads = min(ncores, len(srcs))
 
@@ -185,7 +211,7 @@ def run_reference(a):
         with cf.ThreadPoolExecutor(nthreads) as ex:  # ctypes releases the GIL during the C call
             outs = list(ex.map(lambda s: cpu_sssp_one(h, s), srcs[:nthreads]))
         dt = time.perf_counter() - t0
-        e = sum(int(deg[d != 0xFFFFFFFF].sum()) for d, _ in outs)
+        e = sum(reached_edges(h, d) for d, _ in outs)
         return e, dt, outs[0][1]
 
     for _ in range(a.warmup):
@@ -247,7 +273,6 @@ def run_ours(a):
     nv, ne = h.nv, h.ne
     G = ctx.graph(h)
     dout = torch.empty(nv, dtype=torch.int32, device="cuda")
-    deg = np.diff(h.offsets.astype(np.int64))
 
     # ---- mode selection (the project's autotuner over variant and delta), untimed
     modes = {"hybrid": dict(max_iteration=100000), "push_dd": dict(variant="async_push_dd", max_iteration=100000)}
@@ -328,16 +353,13 @@ def run_ours(a):
     h2d = 4 * (nv + 1) + 8 * ne
     d2h = 4 * nv * len(srcs)
 
-    extra = {}
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(h, srcs)
-    if a.all:
-        extra = run_all(ctx, torch)
     peak, peak_kind = peak_hbm()
     avg_launch_ms = float(np.mean(launch_ms))
     achieved = (step_bytes / len(srcs)) / (avg_launch_ms * 1e-3) / 1e9
-    traffic = read_traffic()
+    traffic = read_traffic(best)
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -351,13 +373,26 @@ def run_ours(a):
         "gpu_launches": a.steps * len(srcs),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "hybrid_engine_kernel<SSSP>",
-                     "avg_launch_ms": avg_launch_ms},
+                     "avg_launch_ms": avg_launch_ms,
+                     "bytes": "4(V+1) + 8*E_reached + 4V per source"},
         "clocks": clk.summary(),
     }
     if cpu:
         line["cpu_baseline"] = cpu
-    if extra:
+    if world == 1 and not a.quick:
+        extra = {}
+        cache = {"rmat22": (h, G)}
+        for name, fn in (("per_algo", per_algo), ("batched", batched), ("served", served)):
+            t0 = time.perf_counter()
+            try:
+                extra[name] = fn(ctx, cache, a)
+            except Exception as e:  # an extra must not hide the headline line
+                extra[name] = {"error": repr(e)}
+            extra[name]["bench_seconds"] = round(time.perf_counter() - t0, 1)
         line["extra"] = extra
+        for k, (_, g) in list(cache.items()):
+            if k != "rmat22":
+                g.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     G.close()
@@ -366,11 +401,11 @@ def run_ours(a):
         torch.distributed.destroy_process_group()
 
 
-def read_traffic():
-    """DRAM bytes per launch of the engine kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "sssp_rmat22_engine_kernel.md")
+def read_traffic(mode):
+    """DRAM bytes per launch of the engine kernel from the committed ncu summary of the selected mode."""
+    name = "sssp_rmat22_delta_engine_kernel.md" if mode.startswith("delta") else "sssp_rmat22_push_dd_engine_kernel.md"
     try:
-        for line in open(p):
+        for line in open(os.path.join(ROOT, "profiles", name)):
             if line.startswith("dram_bytes_per_launch_full_size:"):
                 return float(line.split(":")[1].split()[0])
     except OSError:
@@ -378,30 +413,314 @@ def read_traffic():
     return None
 
 
-def run_all(ctx, torch):
-    """Other configurations, one line each (device time of the engine, median of runs)."""
+# ---------------------------------------------------------------- extras
+def _median_ms(fn, reps, si=1, key="time_kernel_ms"):
+    """Median device time over reps calls (the first dropped when reps > 2); fn()[si] is the sg_stats."""
+    ts, out = [], None
+    for _ in range(reps):
+        out = fn()
+        ts.append(getattr(out[si], key))
+    return statistics.median(ts[1:] if reps > 2 else ts), out
+
+
+def _cpu_time(fn, budget_s=20.0):
+    """Seconds per call of a host function, repeated while under the budget (at least once)."""
+    n, t0 = 0, time.perf_counter()
+    while True:
+        fn()
+        n += 1
+        if time.perf_counter() - t0 > budget_s / 4 or n >= 5:
+            return (time.perf_counter() - t0) / n
+
+
+def _roof(bytes_, ms, peak):
+    gbs = bytes_ / (ms * 1e-3) / 1e9
+    return {"GBs": gbs, "frac_hbm": gbs / peak, "frac_hbm_nominal_8TBs": gbs / 8000.0}
+
+
+def per_algo(ctx, cache, a):
+    """One entry per algorithm: GTEPS, device ms (median of 5 after a warm-up), HBM roofline fraction."""
     import oracle
     import sepgraph as sg
 
+    peak = peak_hbm()[0]
+    ref = oracle.ref_available()
+    cpu_kind = "reference host code compiled from its sources, 1 thread" if ref else "oracle C port, 1 thread"
     res = {}
+    # BFS RMAT-16 symmetric, source = max-degree vertex (the reference's host-checker case)
     h = sg.HostGraph.rmat(16, 16, symmetric=True, seed=1)
     G = ctx.graph(h, symmetric=True)
     src = h.max_degree_vertex()[0]
-    ts = []
-    for _ in range(7):
-        lv, st, _ = G.bfs(src)
-        ts.append(st.time_kernel_ms)
+    t, (lv, st, _) = _median_ms(lambda: G.bfs(src), 6)
     ok = bool((lv == oracle.bfs(h.offsets, h.indices, src)).all())
-    t = statistics.median(ts[2:])
-    t0 = time.perf_counter()
-    oracle.ref_bfs(h.offsets, h.indices, src) if oracle.ref_available() else oracle.bfs(h.offsets, h.indices, src)
-    cpu_s = time.perf_counter() - t0
-    b = 4 * (h.nv + 1) + 4 * st.edges_reached + 4 * h.nv
-    res["bfs_rmat16_sym"] = {"GTEPS": st.edges_reached / t / 1e6, "ms": t, "rounds": st.rounds, "parity": ok,
-                             "frac_hbm": b / (t * 1e-3) / 1e9 / peak_hbm()[0],
-                             "cpu_BFSHost_GTEPS": st.edges_reached / cpu_s / 1e9}
+    cpu_s = _cpu_time(lambda: oracle.ref_bfs(h.offsets, h.indices, src) if ref else oracle.bfs(h.offsets, h.indices, src))
+    res["bfs_rmat16_sym"] = dict(
+        GTEPS=st.edges_reached / t / 1e6, GTEPS_graph500_half_edges=st.edges_reached / 2 / t / 1e6, ms=t,
+        rounds=st.rounds, parity_vs_oracle=ok, **_roof(bfs_bytes(h.nv, st.edges_reached), t, peak),
+        cpu_GTEPS=st.edges_reached / cpu_s / 1e9, cpu_ms=1e3 * cpu_s, cpu=cpu_kind)
+    G.close()
+
+    # SSSP on the 4096x4096 grid, weights [1,1000): delta picked from three candidates, push DD beside
+    h = sg.HostGraph.grid(4096, 4096).gen_weights(1, 1000, 2)
+    G = ctx.graph(h, no_csc=True)
+    src = 0
+    cand = {"push_dd": dict(variant="async_push_dd")}
+    base = max(1, int(32 * float(h.weights.mean()) / (h.ne / h.nv)))
+    for d in (base // 4, base, base * 4):
+        cand[f"delta{max(1, d)}"] = dict(priority="low_high", priority_delta=max(1, d))
+    times, first, agree = {}, None, True
+    for name, kw in cand.items():
+        d, st, _ = G.sssp(src, max_iteration=10000000, **kw)
+        times[name] = st.time_kernel_ms
+        if first is None:
+            first = d.copy()
+        agree &= bool((d == first).all())
+    best = min(times, key=times.get)
+    t, (d, st, _) = _median_ms(lambda: G.sssp(src, max_iteration=10000000, **cand[best]), 6)
+    res["sssp_grid4096_w1-1000"] = dict(
+        GTEPS=st.edges_reached / t / 1e6, ms=t, rounds=st.rounds, mode=best, mode_ms=times, modes_agree=agree,
+        us_per_round=1e3 * t / max(1, st.rounds), **_roof(sssp_bytes(h.nv, st.edges_reached), t, peak),
+        cpu="not timed: the reference's SSSPHostNaive needs about 4 minutes on one core for this graph")
+    G.close()
+    del h, d, first
+
+    # PageRank RMAT-23 directed, FP32, residual 1e-7: data-driven push vs topology-driven pull
+    h = sg.HostGraph.rmat(23, 16, seed=1)
+    G = ctx.graph(h)
+    pr, ranks = {}, {}
+    for v in ("async_push_dd", "sync_pull_td"):
+        t, (r, st, _) = _median_ms(lambda: G.pagerank(variant=v, pr_error=1e-7, max_iteration=100000), 6)
+        if v == "sync_pull_td":
+            b = st.rounds * (4 * (h.nv + 1) + 4 * h.ne + 12 * h.nv)  # gathers assumed L2-served
+            extra = {"bytes_pessimistic_with_gathers": b + st.rounds * 4 * h.ne}
+        else:
+            b = 4 * st.edges_processed + 16 * st.vertices_processed
+            extra = {}
+        pr[v] = dict(ms=t, rounds=st.rounds, edges_processed=st.edges_processed,
+                     GTEPS=st.edges_processed / t / 1e6, **_roof(b, t, peak), **extra)
+        ranks[v] = np.asarray(r, np.float64)
+    p0, p1 = ranks["async_push_dd"], ranks["sync_pull_td"]
+    pr["l1_push_vs_pull_normalised"] = float(np.abs(p0 / p0.sum() - p1 / p1.sum()).sum())
+    G.close()
+    del h, ranks
+    # CPU: PageRankHost at the same threshold on a bounded sample (RMAT-20, same generator)
+    hs = sg.HostGraph.rmat(20, 16, seed=1)
+    cpu_s = _cpu_time(lambda: oracle.ref_pagerank(hs.offsets, hs.indices, 1e-7) if ref
+                      else oracle.pagerank_f32(hs.offsets, hs.indices, 1e-7), budget_s=30.0)
+    Gs = ctx.graph(hs)
+    _, sts, _ = Gs.pagerank(variant="async_push_dd", pr_error=1e-7, max_iteration=100000)
+    pr["cpu"] = {"sample": "RMAT-20 directed (same generator), PageRankHost, 1e-7", "cpu_ms": 1e3 * cpu_s,
+                 "cpu_G_edge_updates_per_s_est": sts.edges_processed / cpu_s / 1e9, "kind": cpu_kind}
+    Gs.close()
+    res["pagerank_rmat23"] = pr
+    del hs
+
+    # BC RMAT-23 symmetrised, source = max-degree vertex
+    h = sg.HostGraph.rmat(23, 16, symmetric=True, seed=1)
+    G = ctx.graph(h, symmetric=True)
+    src = h.max_degree_vertex()[0]
+    t, (bc, sig, st) = _median_ms(lambda: G.bc(src), 6, si=2, key="time_total_ms")
+    e_r = st.edges_reached // 2  # sg_bc counts both traversals
+    b = 2 * (4 * (h.nv + 1) + 4 * e_r) + 32 * h.nv
+    cpu_s = _cpu_time(lambda: oracle.ref_bc(h.offsets, h.indices, src) if ref else oracle.bc_f32(h.offsets, h.indices, src),
+                      budget_s=40.0)
+    res["bc_rmat23_sym"] = dict(GTEPS=2 * e_r / t / 1e6, ms=t, rounds=st.rounds, **_roof(b, t, peak),
+                                cpu_GTEPS=2 * e_r / cpu_s / 1e9, cpu_ms=1e3 * cpu_s, cpu=cpu_kind)
     G.close()
     return res
+
+
+def batched(ctx, cache, a):
+    """Batched launches against one plain launch per query, same results required."""
+    import sepgraph as sg
+
+    res = {}
+    h = sg.HostGraph.rmat(22, 16, symmetric=True, seed=1)
+    G = ctx.graph(h, symmetric=True)
+    srcs = [int(s) for s in h.pick_sources(64, 11)]
+    plain_ms, plain = 0.0, []
+    for s in srcs:
+        lv, st, _ = G.bfs(s)
+        plain_ms += st.time_kernel_ms
+        plain.append(lv)
+    ms_t, (outs, st_t, _) = _median_ms(lambda: ctx.bfs_batch([(G, s) for s in srcs]), 3)
+    same_t = all((o == p).all() for o, p in zip(outs, plain))
+    ms_m, (lv_m, st_m) = _median_ms(lambda: G.msbfs(srcs), 3)
+    same_m = all((lv_m[i] == plain[i]).all() for i in range(len(srcs)))
+    e = sum(reached_edges(h, p) for p in plain)
+    res["bfs64_rmat22_sym"] = {
+        "plain_ms": plain_ms, "plain_qps": 64 / (plain_ms * 1e-3), "plain_GTEPS": e / plain_ms / 1e6,
+        "team_batch_ms": ms_t, "team_batch_qps": 64 / (ms_t * 1e-3), "team_batch_GTEPS": e / ms_t / 1e6,
+        "team_blocks": st_t.vertices_reached, "teams": st_t.search_depth, "team_batch_same_results": same_t,
+        "msbfs_ms": ms_m, "msbfs_qps": 64 / (ms_m * 1e-3), "msbfs_GTEPS": e / ms_m / 1e6, "msbfs_same_results": same_m}
+    del plain, outs, lv_m
+
+    srcs32 = srcs[:32]
+    plain_ms, plain = 0.0, []
+    for s in srcs32:
+        bc, _, st = G.bc(s)
+        plain_ms += st.time_total_ms
+        plain.append(bc)
+    ms_b, (outs, st_b, _) = _median_ms(lambda: ctx.bc_batch([(G, s) for s in srcs32]), 3)
+    same_b = all(np.allclose(o, p, rtol=1e-4, atol=1e-5) for o, p in zip(outs, plain))
+    res["bc32_rmat22_sym"] = {"plain_ms": plain_ms, "plain_qps": 32 / (plain_ms * 1e-3), "batch_ms": ms_b,
+                              "batch_qps": 32 / (ms_b * 1e-3), "same_results_rtol_1e-4": same_b,
+                              "batch_GTEPS": st_b.edges_reached / ms_b / 1e6}
+    G.close()
+    del h, plain, outs
+
+    # 256 SSSP instances over RMAT scale 12-20 graphs (directed, weights [1,64))
+    graphs = []
+    for sc in range(12, 21):
+        hh = sg.HostGraph.rmat(sc, 16, seed=100 + sc).gen_weights(1, 64, 200 + sc)
+        graphs.append((hh, ctx.graph(hh, no_csc=True)))
+    rng = random.Random(5)
+    queries = []
+    for k in range(256):
+        hh, gg = graphs[k % len(graphs)]
+        queries.append((gg, rng.randrange(hh.nv)))
+    kw = dict(variant="async_push_dd", max_iteration=1000000)
+    plain_ms, plain = 0.0, []
+    for gg, s in queries:
+        d, st, _ = gg.sssp(s, **kw)
+        plain_ms += st.time_kernel_ms
+        plain.append(d)
+    ms_s, (outs, st_s, _) = _median_ms(lambda: ctx.sssp_batch(queries, **kw), 3)
+    same_s = all((o == p).all() for o, p in zip(outs, plain))
+    # the same batch planned once and replayed as a CUDA graph into device outputs
+    import torch
+
+    douts = [torch.empty(gg.nv, dtype=torch.int32, device="cuda") for gg, _ in queries]
+    plan = ctx.batch_plan("sssp", queries, douts, **kw)
+    plan_ms = []
+    for _ in range(6):
+        plan.launch()
+        st_p, _ = plan.wait()
+        plan_ms.append(st_p.time_kernel_ms)
+    same_p = all((d.cpu().numpy().view(np.uint32) == p).all() for d, p in zip(douts, plain))
+    captured = plan.captured
+    plan.close()
+    ms_p = statistics.median(plan_ms[1:])
+    res["sssp256_rmat12-20"] = {"plain_ms": plain_ms, "plain_qps": 256 / (plain_ms * 1e-3), "batch_ms": ms_s,
+                                "batch_qps": 256 / (ms_s * 1e-3), "same_results": same_s,
+                                "batch_GTEPS": st_s.edges_reached / ms_s / 1e6, "teams": st_s.search_depth,
+                                "team_blocks": st_s.vertices_reached, "plan_ms": ms_p,
+                                "plan_qps": 256 / (ms_p * 1e-3), "plan_cuda_graph": captured,
+                                "plan_same_results": same_p}
+    for _, gg in graphs:
+        gg.close()
+    return res
+
+
+SERVED_MIX = (("bfs", 0.60), ("sssp", 0.25), ("pagerank", 0.10), ("bc", 0.05))
+
+
+def served(ctx, cache, a):
+    """Mixed query stream through the server vs the plain path on a sample of it."""
+    import sepgraph as sg
+
+    specs = [("rmat", sc) for sc in range(14, 23)] + [("grid", n) for n in (1024, 1448, 2048, 2560, 2896, 3584, 4096)]
+    graphs = []
+    for k, (kind, p) in enumerate(specs):
+        if kind == "rmat" and p == 22 and "rmat22" in cache:
+            hh, gg = cache["rmat22"]  # the headline graph (same generator and weights)
+        elif kind == "rmat":
+            hh = sg.HostGraph.rmat(p, 16, seed=300 + p).gen_weights(1, 64, 400 + p)
+            gg = ctx.graph(hh)
+            cache[f"served_rmat{p}"] = (hh, gg)
+        else:
+            hh = sg.HostGraph.grid(p, p).gen_weights(1, 64, 500 + p)
+            gg = ctx.graph(hh)
+            cache[f"served_grid{p}"] = (hh, gg)
+        graphs.append((f"{kind}{p}", hh, gg))
+    nq = a.served_queries
+    rng = random.Random(17)
+    names, probs = zip(*SERVED_MIX)
+    queries = []
+    for _ in range(nq):
+        algo = rng.choices(names, probs)[0]
+        gid = rng.randrange(len(graphs))
+        nv = graphs[gid][1].nv
+        queries.append((algo, gid, rng.randrange(nv)))
+    sample_every = 10
+    sample = set(range(0, nq, sample_every))
+    # outputs: sampled queries get their own arrays (compared below), the rest share per-graph sinks
+    sinks = {}
+
+    def out_for(i, algo, gid):
+        dt = np.float32 if algo in ("pagerank", "bc") else np.uint32
+        if i in sample:
+            return np.zeros(graphs[gid][1].nv, dt)
+        key = (gid, dt)
+        if key not in sinks:
+            sinks[key] = np.zeros(graphs[gid][1].nv, dt)
+        return sinks[key]
+
+    outs = [out_for(i, al, g) for i, (al, g, _) in enumerate(queries)]
+    rate = 2000.0  # offered load, queries/s (Poisson)
+    srv = sg.Server(0, slots=3, max_batch=256)
+    try:
+        for _, _, gg in graphs:
+            srv.add_graph(gg)
+        tickets = [None] * nq
+        t_start = time.perf_counter()
+
+        def producer():
+            r = random.Random(23)
+            for i, (al, g, s) in enumerate(queries):
+                tickets[i] = srv.submit(al, g, s, outs[i])
+                time.sleep(r.expovariate(rate))
+
+        th = threading.Thread(target=producer)
+        th.start()
+        th.join()
+        statuses = [srv.wait(t, 1800.0) for t in tickets]
+        wall = time.perf_counter() - t_start
+        st = srv.stats()
+    finally:
+        srv.close()
+    failed = sum(1 for s_, _ in statuses if s_ != 0)
+
+    # plain path: the sampled queries one at a time, results to host like the server's
+    plain_lat, same = [], True
+    for i in sorted(sample):
+        al, g, s = queries[i]
+        gg = graphs[g][2]
+        t0 = time.perf_counter()
+        if al == "bfs":
+            o, _, _ = gg.bfs(s, max_iteration=1000000)
+        elif al == "sssp":
+            o, _, _ = gg.sssp(s, variant="async_push_dd", max_iteration=1000000)
+        elif al == "pagerank":
+            o, _, _ = gg.pagerank(pr_error=1e-7, max_iteration=100000)
+        else:
+            o, _, _ = gg.bc(s, max_iteration=1000000)
+        plain_lat.append(1e3 * (time.perf_counter() - t0))
+        if al in ("bfs", "sssp"):
+            same &= bool((o == outs[i]).all())
+        elif al == "pagerank":
+            x, y = np.asarray(o, np.float64), np.asarray(outs[i], np.float64)
+            same &= bool(np.abs(x / x.sum() - y / y.sum()).sum() <= 1e-6)
+        else:
+            same &= bool(np.allclose(o, outs[i], rtol=1e-4, atol=1e-5))
+    plain_lat_sorted = sorted(plain_lat)
+
+    def pct(v, p):
+        return v[min(len(v) - 1, int(p * (len(v) - 1) + 0.5))]
+
+    plain_qps = len(plain_lat) / (sum(plain_lat) * 1e-3)
+    served_qps = nq / wall
+    return {
+        "queries": nq, "offered_qps": rate, "mix": dict(SERVED_MIX), "graphs": [n for n, _, _ in graphs],
+        "served_qps": served_qps, "server_qps_first_to_last": st["qps"], "p50_ms": st["p50_ms"],
+        "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "batches": st["batches"],
+        "failed": failed, "hbm_peak_bytes": st["hbm_peak"], "hbm_budget_bytes": st["hbm_budget"],
+        "plain_sample": len(plain_lat), "plain_qps": plain_qps, "plain_p50_ms": pct(plain_lat_sorted, 0.5),
+        "plain_p99_ms": pct(plain_lat_sorted, 0.99), "speedup_qps": served_qps / plain_qps,
+        "sample_results_same": same,
+        "note": "plain path = one blocking call per query on the sampled 1-in-10 queries, service time only "
+                "(no queueing); served latency includes queueing under the offered Poisson load",
+    }
 
 
 def main():

@@ -207,6 +207,23 @@ sg_status sg_bfs_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const s
 sg_status sg_bc_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt, sg_stats *stats,
                       float *per_query_ms);
 
+/* A batch planned once and launched many times (algo = SG_QUERY_BFS, _SSSP or
+ * _BC): query descriptors, team workspaces (owned by the plan) and outputs are
+ * fixed at creation, and each launch replays one CUDA graph holding the
+ * per-launch memsets and the cooperative kernel on the context's stream (or
+ * issues the same calls directly where the driver cannot capture them;
+ * sg_batch_plan_captured tells which).  Outputs must be device memory.
+ * sg_batch_plan_launch does not wait; sg_batch_plan_wait waits for the last
+ * launch and fills stats / per_query_ms like sg_sssp_batch.  The graphs must
+ * outlive the plan. */
+typedef struct sg_batch_plan sg_batch_plan;
+sg_status sg_batch_plan_create(sg_ctx *ctx, int algo, const sg_batch_query *q, uint32_t n, const sg_options *opt,
+                               sg_batch_plan **out);
+sg_status sg_batch_plan_launch(sg_batch_plan *plan);
+sg_status sg_batch_plan_wait(sg_batch_plan *plan, sg_stats *stats, float *per_query_ms);
+int sg_batch_plan_captured(const sg_batch_plan *plan);
+sg_status sg_batch_plan_destroy(sg_batch_plan *plan);
+
 /* ------------------------------------------------------------------ serving
  * No counterpart in the reference.  A query server over device-resident
  * graphs with continuous batching: `slots` worker threads, each with its own
@@ -255,11 +272,32 @@ sg_status sg_server_get_stats(sg_server *s, sg_server_stats *st);
 sg_status sg_server_reset_stats(sg_server *s);
 sg_status sg_server_destroy(sg_server *s);
 
+/* ------------------------------------------------------------------ autotuner
+ * No counterpart in the reference (its variants, thresholds and grid shape are
+ * command-line choices).  Times a fixed set of candidate options for one
+ * algorithm (SG_QUERY_*) on the given graph and sources — variant (hybrid
+ * policy, forced push, forced pull), SSSP two-level priority delta around the
+ * reference heuristic 32*avg_w/avg_deg, blocks per SM and the heavy-vertex
+ * split threshold — checks that every candidate gives the same result as the
+ * first (bit-exact for BFS/SSSP, L1 <= 1e-6 for PageRank, 1e-4 relative for
+ * BC) and writes the fastest to *best (starting from *base, NULL = defaults).
+ * report (optional) receives one line per candidate; at most max_candidates
+ * entries are timed (0 = all). */
+typedef struct sg_tune_entry {
+    sg_options options;
+    double ms;       /* median device time per source */
+    int32_t status;  /* sg_status of the candidate; SG_ERR_FORMAT if its result differed */
+    int32_t pad;
+} sg_tune_entry;
+sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources, uint32_t nsrc, const sg_options *base,
+                      uint32_t max_candidates, sg_options *best, double *best_ms, sg_tune_entry *report,
+                      uint32_t report_capacity, uint32_t *n_report);
+
 /* BFS that allocates nothing, for callers that cannot call cudaMalloc (code
  * running inside another framework's memory pool or under a device-memory
  * budget).  No counterpart in the reference.  Runs the sg_bfs engine on the
  * calling thread's current device with every worklist, bitmap and control word
- * in one fixed file-scope device array (about 13 MB, held by every GPU that
+ * in one fixed file-scope device array (about 19 MB, held by every GPU that
  * loads it until exit).  Limits: nv <= 262144 vertices, ne <= 8388608 edges;
  * larger graphs return SG_ERR_CAPACITY before any work.  offsets/indices (CSR),
  * optional in_offsets/in_indices (CSC; pass the CSR again for a symmetric

@@ -1,0 +1,165 @@
+// Autotuner over engine options (declaration and contract in
+// include/sepgraph.h, "autotuner").  Host code over the public entry points:
+// every candidate runs the real engine on the caller's graph and sources and
+// must reproduce the first candidate's result before its time counts.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../../include/sepgraph.h"
+#include "../sg_internal.h"
+
+namespace {
+
+std::vector<sg_options> candidates(sg_graph *g, int algo, const sg_options &base) {
+    std::vector<sg_options> out;
+    auto add = [&](int variant, int bps, int heavy, int priority, double delta) {
+        sg_options o = base;
+        o.variant = variant;
+        o.blocks_per_sm = bps;
+        o.heavy_degree = heavy;
+        o.priority = priority;
+        o.priority_delta = delta;
+        o.blocking = 1;
+        out.push_back(o);
+    };
+    const int bps_set[] = {2, 4, 8};
+    if (algo == SG_QUERY_BFS) {
+        for (int v : {SG_VARIANT_AUTO, SG_ASYNC_PUSH_DD})
+            for (int b : {1, 2, 4, 8})
+                for (int hv : {32, 128}) add(v, b, hv, SG_PRIORITY_NONE, 0);
+    } else if (algo == SG_QUERY_SSSP) {
+        uint32_t nv = 0;
+        uint64_t ne = 0;
+        sg_graph_info(g, &nv, &ne, nullptr, nullptr);
+        const double avg_w = ne ? sgb::graph_weight_sum(g) / (double)ne : 1.0;
+        const double avg_deg = nv ? (double)ne / nv : 1.0;
+        const double heuristic = std::max(1.0, std::floor(32.0 * avg_w / std::max(avg_deg, 1e-9)));  // hybrid_sssp.cu:196-197
+        for (int b : bps_set) {
+            add(SG_VARIANT_AUTO, b, 0, SG_PRIORITY_NONE, 0);
+            add(SG_ASYNC_PUSH_DD, b, 0, SG_PRIORITY_NONE, 0);
+            for (double f : {1.0 / 16, 1.0 / 4, 1.0, 4.0})
+                add(SG_ASYNC_PUSH_DD, b, 0, SG_PRIORITY_LOW_HIGH, std::max(1.0, std::floor(heuristic * f)));
+        }
+    } else if (algo == SG_QUERY_PAGERANK) {
+        for (int v : {SG_VARIANT_AUTO, SG_SYNC_PULL_TD, SG_ASYNC_PUSH_DD})
+            for (int b : bps_set) add(v, b, 0, SG_PRIORITY_NONE, 0);
+    } else {
+        for (int v : {SG_VARIANT_AUTO, SG_ASYNC_PUSH_DD})
+            for (int b : bps_set) add(v, b, 0, SG_PRIORITY_NONE, 0);
+    }
+    return out;
+}
+
+struct Result {
+    std::vector<uint32_t> u;
+    std::vector<float> f;
+};
+
+sg_status run_one(sg_graph *g, int algo, uint32_t src, const sg_options &o, uint32_t nv, Result &r, double *ms) {
+    sg_stats st;
+    std::memset(&st, 0, sizeof st);
+    sg_status s;
+    if (algo == SG_QUERY_BFS || algo == SG_QUERY_SSSP) {
+        r.u.resize(nv);
+        s = algo == SG_QUERY_BFS ? sg_bfs(g, src, &o, r.u.data(), &st) : sg_sssp(g, src, &o, r.u.data(), &st);
+        *ms = st.time_kernel_ms;
+    } else if (algo == SG_QUERY_PAGERANK) {
+        r.f.resize(nv);
+        s = sg_pagerank(g, &o, r.f.data(), nullptr, &st);
+        *ms = st.time_kernel_ms;
+    } else {
+        r.f.resize(nv);
+        s = sg_bc(g, src, &o, r.f.data(), nullptr, &st);
+        *ms = st.time_total_ms;
+    }
+    if (s == SG_OK && st.max_iteration_reached) s = SG_ERR_CAPACITY;  // an unfinished run is not a result
+    return s;
+}
+
+// Same result within the algorithm's tolerance: BFS/SSSP exact; PageRank L1 of
+// the L1-normalised vectors within max(1e-6, 20 * residual threshold); BC 1e-4
+// relative + 1e-5 absolute.
+bool same(int algo, const Result &a, const Result &b, double pr_error) {
+    if (algo == SG_QUERY_BFS || algo == SG_QUERY_SSSP) return a.u == b.u;
+    if (a.f.size() != b.f.size()) return false;
+    if (algo == SG_QUERY_PAGERANK) {
+        double sa = 0, sb = 0, l1 = 0;
+        for (size_t i = 0; i < a.f.size(); ++i) {
+            sa += a.f[i];
+            sb += b.f[i];
+        }
+        if (sa <= 0 || sb <= 0) return false;
+        for (size_t i = 0; i < a.f.size(); ++i) l1 += std::fabs(a.f[i] / sa - b.f[i] / sb);
+        return l1 <= std::max(1e-6, 20.0 * pr_error);
+    }
+    for (size_t i = 0; i < a.f.size(); ++i)
+        if (std::fabs((double)a.f[i] - b.f[i]) > 1e-5 + 1e-4 * std::fabs((double)b.f[i])) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources, uint32_t nsrc, const sg_options *base,
+                                 uint32_t max_candidates, sg_options *best, double *best_ms, sg_tune_entry *report,
+                                 uint32_t report_capacity, uint32_t *n_report) {
+    if (!g || !best || algo < SG_QUERY_BFS || algo > SG_QUERY_BC) return SG_ERR_INVALID_ARG;
+    uint32_t nv = 0;
+    sg_status st = sg_graph_info(g, &nv, nullptr, nullptr, nullptr);
+    if (st != SG_OK) return st;
+    const bool sourceless = algo == SG_QUERY_PAGERANK;
+    if (!sourceless && (!sources || nsrc == 0)) return SG_ERR_INVALID_ARG;
+    for (uint32_t i = 0; !sourceless && i < nsrc; ++i)
+        if (sources[i] >= nv) return SG_ERR_INVALID_ARG;
+    sg_options b0;
+    if (base)
+        b0 = *base;
+    else
+        sg_options_default(&b0);
+    std::vector<sg_options> cand = candidates(g, algo, b0);
+    if (max_candidates && cand.size() > max_candidates) cand.resize(max_candidates);
+    const uint32_t runs = sourceless ? 1u : nsrc;
+    std::vector<Result> ref(runs);
+    bool have_ref = false;
+    double best_t = -1;
+    if (n_report) *n_report = 0;
+    for (size_t c = 0; c < cand.size(); ++c) {
+        std::vector<double> ts;
+        sg_status cs = SG_OK;
+        std::vector<Result> res(runs);
+        for (uint32_t k = 0; k < runs && cs == SG_OK; ++k) {
+            double ms = 0;
+            cs = run_one(g, algo, sourceless ? 0u : sources[k], cand[c], nv, res[k], &ms);
+            ts.push_back(ms);
+        }
+        if (cs == SG_OK) {
+            if (!have_ref) {
+                ref = res;
+                have_ref = true;
+            } else {
+                for (uint32_t k = 0; k < runs; ++k)
+                    if (!same(algo, res[k], ref[k], b0.pr_error)) cs = SG_ERR_FORMAT;
+            }
+        }
+        double med = 0;
+        if (!ts.empty()) {
+            std::sort(ts.begin(), ts.end());
+            med = ts[ts.size() / 2];
+        }
+        if (cs == SG_OK && (best_t < 0 || med < best_t)) {
+            best_t = med;
+            *best = cand[c];
+        }
+        if (report && n_report && *n_report < report_capacity) {
+            sg_tune_entry &e = report[(*n_report)++];
+            e.options = cand[c];
+            e.ms = med;
+            e.status = cs;
+            e.pad = 0;
+        }
+    }
+    if (best_t < 0) return SG_ERR_UNSUPPORTED;  // no candidate finished
+    if (best_ms) *best_ms = best_t;
+    return SG_OK;
+}

@@ -410,6 +410,7 @@ sg_status sg_graph_destroy(sg_graph *g) {
 }  // extern "C"
 
 sg_ctx *sgb::graph_context(const sg_graph *g) { return g ? g->ctx : nullptr; }
+double sgb::graph_weight_sum(const sg_graph *g) { return g ? g->weight_sum : 0.0; }
 
 extern "C" {
 

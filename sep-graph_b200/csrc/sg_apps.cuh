@@ -23,6 +23,7 @@ constexpr uint32_t kInf = 0xffffffffu;  // IDENTITY_ELEMENT of BFS/SSSP/BC (UINT
 template <typename TValue, typename TBuffer, typename TWeight, typename... Unused>
 struct BFS : AppBase<TValue, TBuffer, TWeight> {
     using AppBase<TValue, TBuffer, TWeight>::AccumulateBuffer;
+    static constexpr bool kReorderSafe = true;  // result independent of push order
     index_t m_source_node;
     bool m_non_atomic;
 
@@ -77,6 +78,7 @@ struct BFS : AppBase<TValue, TBuffer, TWeight> {
 template <typename TValue, typename TBuffer, typename TWeight, typename... Unused>
 struct SSSP : AppBase<TValue, TBuffer, TWeight> {
     using AppBase<TValue, TBuffer, TWeight>::AccumulateBuffer;
+    static constexpr bool kReorderSafe = true;  // result independent of push order
     index_t m_source_node;
 
     explicit SSSP(index_t source) : m_source_node(source) {}
@@ -120,6 +122,7 @@ struct SSSP : AppBase<TValue, TBuffer, TWeight> {
 template <typename TValue, typename TBuffer, typename TWeight, typename... Unused>
 struct PageRank : AppBase<TValue, TBuffer, TWeight> {
     using AppBase<TValue, TBuffer, TWeight>::AccumulateBuffer;
+    static constexpr bool kReorderSafe = true;  // result independent of push order
     double m_error;
 
     explicit PageRank(double error) : m_error(error) {}

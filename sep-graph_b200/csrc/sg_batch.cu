@@ -500,24 +500,61 @@ __global__ void __launch_bounds__(engine::kBlockThreads)
 }
 
 template <typename T>
-sg_status ws_get(sg_ctx *ctx, const char *name, size_t n, T **out) {
-    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace;
-    SG_TRY_CUDA(ctx, ctx->batch_ws->get(name, n, out));
+sg_status ws_get(sg_ctx *ctx, sgb::Workspace &ws, const char *name, size_t n, T **out) {
+    SG_TRY_CUDA(ctx, ws.get(name, n, out));
     return SG_OK;
 }
 
-// Runs n queries of one functor type in one batched launch.  outs[i] receives
-// query i's value array (host or device memory of nv_i elements).
+// Everything one batched launch needs once its descriptors are on the device:
+// the kernel, its grid and argument values (their addresses are the launch's
+// argument array, so a Build must stay put while it is enqueued or captured),
+// the buffers to zero before each launch and the host-side bookkeeping.
+struct BatchBuild {
+    const void *kernel = nullptr;
+    uint32_t n = 0, n_teams = 0, team_blocks = 0;
+    void *dq = nullptr, *dsp = nullptr, *dbc = nullptr, *douts = nullptr;
+    uint32_t *counter = nullptr;
+    engine::BatchResult *dres = nullptr;
+    engine::Params p{};
+    void *args[9] = {};
+    struct Zero {
+        void *ptr;
+        size_t bytes;
+    };
+    std::vector<Zero> zero;
+    std::vector<uint32_t> order;         // launch position -> query index
+    std::vector<sg_graph *> graphs;      // by query index
+    std::vector<void *> outs, vptr;      // caller output, device array written by the kernel
+    std::vector<bool> out_dev;
+    bool bc = false;
+    size_t value_bytes = 4;
+};
+
+// Zeroes the per-launch state and launches; no host synchronisation (capturable).
+sg_status enqueue_batch(sg_ctx *ctx, BatchBuild &B, cudaStream_t s) {
+    for (auto &z : B.zero) SG_TRY_CUDA(ctx, cudaMemsetAsync(z.ptr, 0, z.bytes, s));
+    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel(B.kernel, dim3(B.n_teams * B.team_blocks), dim3(engine::kBlockThreads),
+                                                 B.args, 0, s));
+    return SG_OK;
+}
+
+// Plans n queries of one functor type as one batched launch: team sizing,
+// team workspaces and query descriptors in `ws`, outputs in place (device) or
+// through a staging array (host).  With device_outputs_only, host outputs are
+// rejected (a captured launch cannot copy to pageable memory).
 template <typename App, typename TV, typename TB, typename TW>
-sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, const std::vector<sg_graph *> &graphs,
-                    const std::vector<void *> &outs, const sg_options &o, engine::Params p, sg_stats *stats,
-                    float *per_query_ms) {
+sg_status prepare_batch(sg_ctx *ctx, sgb::Workspace &ws, std::vector<engine::BatchQuery<App, TV>> qs,
+                        const std::vector<sg_graph *> &graphs, const std::vector<void *> &outs, const sg_options &o,
+                        engine::Params p, bool device_outputs_only, BatchBuild &B) {
     using namespace engine;
     const uint32_t n = (uint32_t)qs.size();
+    B.n = n;
+    B.graphs = graphs;
+    B.outs = outs;
     // largest graphs first (longest-processing-time order)
-    std::vector<uint32_t> order(n);
-    for (uint32_t i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return graphs[x]->ne > graphs[y]->ne; });
+    B.order.resize(n);
+    for (uint32_t i = 0; i < n; ++i) B.order[i] = i;
+    std::stable_sort(B.order.begin(), B.order.end(), [&](uint32_t x, uint32_t y) { return graphs[x]->ne > graphs[y]->ne; });
     uint32_t nv_max = 0;
     uint64_t ne_max = 0;
     for (auto *g : graphs) {
@@ -525,9 +562,11 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
         ne_max = std::max(ne_max, g->ne);
     }
     constexpr bool kBC = std::is_same<App, BCApp>::value;
-    const void *kernel = kBC ? (const void *)batched_bc_kernel : (const void *)batched_engine_kernel<App, TV, TB, TW>;
+    B.bc = kBC;
+    B.value_bytes = sizeof(TV);
+    B.kernel = kBC ? (const void *)batched_bc_kernel : (const void *)batched_engine_kernel<App, TV, TB, TW>;
     static int max_bps = 0;
-    if (!max_bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_bps, kernel, kBlockThreads, 0));
+    if (!max_bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_bps, B.kernel, kBlockThreads, 0));
     const int bps = std::max(1, std::min(max_bps, o.blocks_per_sm > 0 ? o.blocks_per_sm : 4));
     const uint32_t total_blocks = (uint32_t)(ctx->prop.multiProcessorCount * bps);
     // Automatic team size: one block per 2M edges of the largest graph (64
@@ -541,6 +580,8 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
     }
     team_blocks = std::max(1u, std::min(team_blocks, total_blocks));
     const uint32_t n_teams = std::max(1u, std::min(n, total_blocks / team_blocks));
+    B.team_blocks = team_blocks;
+    B.n_teams = n_teams;
 
     // team workspaces
     const uint32_t nwords = nv_max / 32 + 1;
@@ -552,20 +593,22 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
     Ctrl *ctrl;
     const size_t T = n_teams;
     sg_status st;
-    if ((st = ws_get(ctx, "b_buf", T * nv_max * sizeof(TB) / sizeof(TB), &buf)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_tmp", T * nv_max, &tmp)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_q", T * 3 * nv_max, &qq)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_bm", T * 2 * nwords, &bm)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_fl", T * 3 * nwords, &fl)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_mid", T * nv_max, &mid)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_heavy", T * heavy_cap, &heavy)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_chunk", T * chunk_cap, &chunk)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_ctrl", T, &ctrl)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_counter", 1, &counter)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_buf", T * nv_max, &buf)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_tmp", T * nv_max, &tmp)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_q", T * 3 * nv_max, &qq)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_bm", T * 2 * nwords, &bm)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_fl", T * 3 * nwords, &fl)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_mid", T * nv_max, &mid)) != SG_OK) return st;
+    // two heavy-vertex tables per team (one per round parity)
+    if ((st = ws_get(ctx, ws, "b_heavy", T * 2 * heavy_cap, &heavy)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_chunk", T * 2 * chunk_cap, &chunk)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_ctrl", T, &ctrl)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_counter", 1, &counter)) != SG_OK) return st;
     // heavy/chunk tables start zeroed so that a stale chunk never names an out-of-range item
-    SG_TRY_CUDA(ctx, cudaMemsetAsync(heavy, 0, T * heavy_cap * sizeof(HeavyItem<TB>), ctx->stream));
-    SG_TRY_CUDA(ctx, cudaMemsetAsync(ctrl, 0, T * sizeof(Ctrl), ctx->stream));
-    SG_TRY_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), ctx->stream));
+    B.zero.push_back({heavy, T * 2 * heavy_cap * sizeof(HeavyItem<TB>)});
+    B.zero.push_back({ctrl, T * sizeof(Ctrl)});
+    B.zero.push_back({counter, sizeof(uint32_t)});
+    B.counter = counter;
     std::vector<TeamSpace<TB>> spaces(T);
     for (size_t t = 0; t < T; ++t) {
         TeamSpace<TB> &s = spaces[t];
@@ -578,8 +621,8 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
         s.bitmap[0] = bm + (t * 2) * nwords;
         s.bitmap[1] = bm + (t * 2 + 1) * nwords;
         s.middle = mid + t * nv_max;
-        s.heavy = heavy + t * heavy_cap;
-        s.chunk_owner = chunk + t * chunk_cap;
+        s.heavy = heavy + t * 2 * heavy_cap;
+        s.chunk_owner = chunk + t * 2 * chunk_cap;
         s.ctrl = ctrl + t;
         s.trace = nullptr;
         s.cap_v = nv_max;
@@ -588,8 +631,6 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
         s.trace_cap = 0;
     }
     // BC: levels, path counts, dependencies, level stack and chunk table per team
-    BCTeam *dbc = nullptr;
-    float **douts = nullptr;
     if constexpr (kBC) {
         const uint32_t max_levels = std::min(p.max_iteration, nv_max) + 2;  // a level holds at least one vertex
         const uint32_t bchunk_cap = (uint32_t)(ne_max / bc::kBcChunk + ne_max / bc::kBcBigDegree + 2);
@@ -597,96 +638,113 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
         unsigned long long *sig;
         float *dl;
         uint4 *bch;
-        if ((st = ws_get(ctx, "bc_level", T * nv_max, &lv)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "bc_sigma", T * nv_max, &sig)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "bc_delta", T * nv_max, &dl)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "bc_stack", T * nv_max, &stk)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "bc_ends", T * max_levels, &ends)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "bc_ccount", T * max_levels, &cc)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "bc_misc", T * 4, &misc)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "bc_chunks", T * bchunk_cap, &bch)) != SG_OK) return st;
+        BCTeam *dbc;
+        if ((st = ws_get(ctx, ws, "bc_level", T * nv_max, &lv)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_sigma", T * nv_max, &sig)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_delta", T * nv_max, &dl)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_stack", T * nv_max, &stk)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_ends", T * max_levels, &ends)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_ccount", T * max_levels, &cc)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_misc", T * 4, &misc)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_chunks", T * bchunk_cap, &bch)) != SG_OK) return st;
         std::vector<BCTeam> bts(T);
         for (size_t t = 0; t < T; ++t)
             bts[t] = BCTeam{lv + t * nv_max, sig + t * nv_max, dl + t * nv_max, stk + t * nv_max, ends + t * max_levels,
                             misc + t * 4, cc + t * max_levels, bch + t * bchunk_cap, bchunk_cap, max_levels};
-        if ((st = ws_get(ctx, "bc_teams", T, &dbc)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "bc_teams", T, &dbc)) != SG_OK) return st;
         SG_TRY_CUDA(ctx, cudaMemcpyAsync(dbc, bts.data(), T * sizeof(BCTeam), cudaMemcpyHostToDevice, ctx->stream));
+        B.dbc = dbc;
     }
     // outputs: device outputs are written in place, host outputs go through a staging array
-    std::vector<bool> out_dev(n);
+    B.out_dev.assign(n, false);
     TV *stage = nullptr;
     size_t stage_elems = 0;
     for (uint32_t i = 0; i < n; ++i) {
-        out_dev[i] = sgb::is_device_ptr(outs[i], ctx->device);
-        if (!out_dev[i]) stage_elems += graphs[i]->nv;
+        B.out_dev[i] = sgb::is_device_ptr(outs[i], ctx->device);
+        if (!B.out_dev[i]) {
+            if (device_outputs_only) return sgb::set_error(ctx, SG_ERR_INVALID_ARG, "batch plan output %u is not device memory", i);
+            stage_elems += graphs[i]->nv;
+        }
     }
-    if (stage_elems && (st = ws_get(ctx, "b_stage", stage_elems, &stage)) != SG_OK) return st;
-    std::vector<TV *> vptr(n);
+    if (stage_elems && (st = ws_get(ctx, ws, "b_stage", stage_elems, &stage)) != SG_OK) return st;
+    B.vptr.assign(n, nullptr);
     {
         size_t off = 0;
         for (uint32_t i = 0; i < n; ++i) {
-            vptr[i] = out_dev[i] ? (TV *)outs[i] : stage + off;
-            if (!out_dev[i]) off += graphs[i]->nv;
+            B.vptr[i] = B.out_dev[i] ? outs[i] : (void *)(stage + off);
+            if (!B.out_dev[i]) off += graphs[i]->nv;
         }
     }
     std::vector<BatchQuery<App, TV>> qd;
     qd.reserve(n);
     std::vector<float *> fouts(n);
     for (uint32_t k = 0; k < n; ++k) {
-        qd.push_back(qs[order[k]]);
-        qd.back().value = vptr[order[k]];
-        fouts[k] = reinterpret_cast<float *>(vptr[order[k]]);  // BC writes 4-byte floats in the same slots
+        qd.push_back(qs[B.order[k]]);
+        qd.back().value = (TV *)B.vptr[B.order[k]];
+        fouts[k] = reinterpret_cast<float *>(B.vptr[B.order[k]]);  // BC writes 4-byte floats in the same slots
     }
     if constexpr (kBC) {
-        if ((st = ws_get(ctx, "bc_outs", n, &douts)) != SG_OK) return st;
+        float **douts;
+        if ((st = ws_get(ctx, ws, "bc_outs", n, &douts)) != SG_OK) return st;
         SG_TRY_CUDA(ctx, cudaMemcpyAsync(douts, fouts.data(), n * sizeof(float *), cudaMemcpyHostToDevice, ctx->stream));
+        B.douts = douts;
     }
     BatchQuery<App, TV> *dq;
     TeamSpace<TB> *dsp;
-    BatchResult *dres;
-    if ((st = ws_get(ctx, "b_queries", n, &dq)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_spaces", T, &dsp)) != SG_OK) return st;
-    if ((st = ws_get(ctx, "b_results", n, &dres)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_queries", n, &dq)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_spaces", T, &dsp)) != SG_OK) return st;
+    if ((st = ws_get(ctx, ws, "b_results", n, &B.dres)) != SG_OK) return st;
     SG_TRY_CUDA(ctx, cudaMemcpyAsync(dq, qd.data(), n * sizeof(qd[0]), cudaMemcpyHostToDevice, ctx->stream));
     SG_TRY_CUDA(ctx, cudaMemcpyAsync(dsp, spaces.data(), T * sizeof(spaces[0]), cudaMemcpyHostToDevice, ctx->stream));
-    SG_TRY_CUDA(ctx, cudaMemsetAsync(dres, 0, n * sizeof(BatchResult), ctx->stream));
-    uint32_t tb = team_blocks;
-    void *args[] = {(void *)&dq, (void *)&n, (void *)&dsp, (void *)&tb, (void *)&counter, (void *)&dres, (void *)&p};
-    void *bc_args[] = {(void *)&dq,  (void *)&n,       (void *)&dsp,  (void *)&dbc, (void *)&douts,
-                       (void *)&tb,  (void *)&counter, (void *)&dres, (void *)&p};
-    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel(kernel, dim3(n_teams * team_blocks), dim3(kBlockThreads),
-                                                 kBC ? bc_args : args, 0, ctx->stream));
-    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
-    if (!o.blocking) return SG_OK;
+    B.zero.push_back({B.dres, n * sizeof(BatchResult)});
+    B.dq = dq;
+    B.dsp = dsp;
+    B.p = p;
+    if (kBC) {
+        void *a[] = {&B.dq, &B.n, &B.dsp, &B.dbc, &B.douts, &B.team_blocks, &B.counter, &B.dres, &B.p};
+        std::copy(a, a + 9, B.args);
+    } else {
+        void *a[] = {&B.dq, &B.n, &B.dsp, &B.team_blocks, &B.counter, &B.dres, &B.p};
+        std::copy(a, a + 7, B.args);
+    }
+    return SG_OK;
+}
+
+// After a launch: outputs to the host, per-query results, aggregate stats.
+sg_status finish_batch(sg_ctx *ctx, sgb::Workspace &ws, BatchBuild &B, bool copy_outputs, sg_stats *stats,
+                       float *per_query_ms) {
+    using namespace engine;
+    const uint32_t n = B.n;
+    sg_status st;
     std::vector<BatchResult> res(n);
-    SG_TRY_CUDA(ctx, cudaMemcpyAsync(res.data(), dres, n * sizeof(BatchResult), cudaMemcpyDeviceToHost, ctx->stream));
-    for (uint32_t i = 0; i < n; ++i)
-        if (!out_dev[i])
-            SG_TRY_CUDA(ctx, cudaMemcpyAsync(outs[i], vptr[i], graphs[i]->nv * sizeof(TV), cudaMemcpyDeviceToHost,
-                                             ctx->stream));
+    SG_TRY_CUDA(ctx, cudaMemcpyAsync(res.data(), B.dres, n * sizeof(BatchResult), cudaMemcpyDeviceToHost, ctx->stream));
+    if (copy_outputs)
+        for (uint32_t i = 0; i < n; ++i)
+            if (!B.out_dev[i])
+                SG_TRY_CUDA(ctx, cudaMemcpyAsync(B.outs[i], B.vptr[i], B.graphs[i]->nv * B.value_bytes,
+                                                 cudaMemcpyDeviceToHost, ctx->stream));
     // reached edges per query (GTEPS numerator)
     unsigned long long reached = 0;
-    if (stats && !kBC) {
+    if (stats && !B.bc) {
         const uint32_t **rows, **vals;
         uint32_t *nvs;
         unsigned long long *dr;
-        if ((st = ws_get(ctx, "b_rows", n, (const uint32_t ***)&rows)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "b_vals", n, (const uint32_t ***)&vals)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "b_nvs", n, &nvs)) != SG_OK) return st;
-        if ((st = ws_get(ctx, "b_reach", n, &dr)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "b_rows", n, (const uint32_t ***)&rows)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "b_vals", n, (const uint32_t ***)&vals)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "b_nvs", n, &nvs)) != SG_OK) return st;
+        if ((st = ws_get(ctx, ws, "b_reach", n, &dr)) != SG_OK) return st;
         std::vector<const uint32_t *> hr(n), hv(n);
         std::vector<uint32_t> hn(n);
         for (uint32_t i = 0; i < n; ++i) {
-            hr[i] = graphs[i]->row;
-            hv[i] = (const uint32_t *)vptr[i];
-            hn[i] = graphs[i]->nv;
+            hr[i] = B.graphs[i]->row;
+            hv[i] = (const uint32_t *)B.vptr[i];
+            hn[i] = B.graphs[i]->nv;
         }
         SG_TRY_CUDA(ctx, cudaMemcpyAsync(rows, hr.data(), n * sizeof(void *), cudaMemcpyHostToDevice, ctx->stream));
         SG_TRY_CUDA(ctx, cudaMemcpyAsync(vals, hv.data(), n * sizeof(void *), cudaMemcpyHostToDevice, ctx->stream));
         SG_TRY_CUDA(ctx, cudaMemcpyAsync(nvs, hn.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
         SG_TRY_CUDA(ctx, cudaMemsetAsync(dr, 0, n * sizeof(unsigned long long), ctx->stream));
-        if (sizeof(TV) == 4) {
+        if (B.value_bytes == 4) {
             batch_reach_kernel<<<dim3(64, n), 256, 0, ctx->stream>>>(rows, vals, nvs, dr);
             SG_TRY_CUDA(ctx, cudaGetLastError());
         }
@@ -702,9 +760,9 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
     uint32_t bits = 0;
     std::vector<BatchResult> byq(n);
     for (uint32_t k = 0; k < n; ++k) {
-        byq[order[k]] = res[k];
+        byq[B.order[k]] = res[k];
         bits |= res[k].error;
-        if (kBC) reached += 2 * res[k].reached;  // two traversals, as for a single BC query
+        if (B.bc) reached += 2 * res[k].reached;  // two traversals, as for a single BC query
     }
     if (stats) {
         std::memset(stats->rounds_by_variant, 0, sizeof stats->rounds_by_variant);
@@ -721,14 +779,31 @@ sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, co
         stats->edges_reached = reached;
         stats->vertices_processed = n;  // queries in the batch
         stats->device_error = bits;
-        stats->search_depth = n_teams;  // teams used
-        stats->vertices_reached = team_blocks;
+        stats->search_depth = B.n_teams;  // teams used
+        stats->vertices_reached = B.team_blocks;
     }
     if (per_query_ms)
         for (uint32_t i = 0; i < n; ++i) per_query_ms[i] = (float)((byq[i].t_end - byq[i].t_start) * 1e-6);
     const sg_status dst = sgb::device_error_status(bits);
     if (dst != SG_OK) return sgb::set_error(ctx, dst, "batch device error bits 0x%x", bits);
     return SG_OK;
+}
+
+// Runs n queries of one functor type in one batched launch.  outs[i] receives
+// query i's value array (host or device memory of nv_i elements).
+template <typename App, typename TV, typename TB, typename TW>
+sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, const std::vector<sg_graph *> &graphs,
+                    const std::vector<void *> &outs, const sg_options &o, engine::Params p, sg_stats *stats,
+                    float *per_query_ms) {
+    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace;
+    BatchBuild B;
+    sg_status st = prepare_batch<App, TV, TB, TW>(ctx, *ctx->batch_ws, std::move(qs), graphs, outs, o, p, false, B);
+    if (st != SG_OK) return st;
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    if ((st = enqueue_batch(ctx, B, ctx->stream)) != SG_OK) return st;
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    if (!o.blocking) return SG_OK;
+    return finish_batch(ctx, *ctx->batch_ws, B, true, stats, per_query_ms);
 }
 
 engine::Params batch_params(const sg_options &o, int scheme) {
@@ -753,7 +828,7 @@ engine::Params batch_params(const sg_options &o, int scheme) {
 
 template <typename App>
 engine::BatchQuery<App, uint32_t> make_query(App app, sg_graph *g) {
-    engine::BatchQuery<App, uint32_t> bq{app, {}, {}, nullptr, nullptr, nullptr};
+    engine::BatchQuery<App, uint32_t> bq{app, {}, {}, nullptr, nullptr, nullptr, 0ull};
     bq.csr.nnodes = g->nv;
     bq.csr.nedges = (uint32_t)g->ne;
     bq.csr.row_start = g->row;
@@ -774,6 +849,13 @@ engine::BatchQuery<App, uint32_t> make_query(App app, sg_graph *g) {
     app.m_nedges = (uint32_t)g->ne;
     bq.app = app;
     return bq;
+}
+
+// The reference's delta heuristic, 32 * average weight / average degree
+// (samples/hybrid_sssp/hybrid_sssp.cu:196-197), at least 1.
+double default_sssp_delta(const sg_graph *g) {
+    if (!g->ne) return 1.0;
+    return std::max(1.0, std::floor(32.0 * (g->weight_sum / g->ne) / ((double)g->ne / g->nv)));
 }
 
 sg_status check_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n) {
@@ -798,75 +880,133 @@ struct DevGuard {
     }
 };
 
+// Builds the functors and launch parameters of a batch of one algorithm
+// (SG_QUERY_BFS / SSSP / BC) and hands them to `run`, whose
+// go<App, TV, TB, TW>(queries, graphs, outputs, params) plans or runs them.
+template <typename Run>
+sg_status dispatch_batch(int algo, const sg_batch_query *q, uint32_t n, const sg_options &o, Run &run) {
+    engine::Params p = batch_params(o, 0);
+    std::vector<sg_graph *> graphs(n);
+    std::vector<void *> outs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        graphs[i] = q[i].graph;
+        outs[i] = q[i].out;
+        if (!q[i].graph->has_csc && p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
+    }
+    auto build = [&](auto make_app, auto *tag) {
+        using App = std::remove_pointer_t<decltype(tag)>;
+        std::vector<engine::BatchQuery<App, uint32_t>> qs;
+        qs.reserve(n);
+        for (uint32_t i = 0; i < n; ++i) qs.push_back(make_query(make_app(q[i].source), q[i].graph));
+        return qs;
+    };
+    if (algo == SG_QUERY_SSSP) {
+        using App = apps::SSSP<uint32_t, uint32_t, uint32_t>;
+        auto qs = build([](uint32_t s) { return App(s); }, (App *)nullptr);
+        if (o.priority == SG_PRIORITY_LOW_HIGH) {
+            // a given delta for every query, else the reference heuristic on each query's own graph
+            p.priority = 1;
+            if (o.priority_delta > 0)
+                p.prio_init_raw = p.prio_step_raw = engine::to_raw<uint32_t>((uint32_t)o.priority_delta);
+            for (uint32_t i = 0; i < n; ++i) {
+                const sg_graph *g = graphs[i];
+                const double delta = o.priority_delta > 0 ? o.priority_delta : default_sssp_delta(g);
+                qs[i].prio_raw = engine::to_raw<uint32_t>((uint32_t)delta);
+            }
+            if (p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
+            p.collect = 0;
+        }
+        return run.template go<App, uint32_t, uint32_t, uint32_t>(qs, graphs, outs, p);
+    }
+    if (algo == SG_QUERY_BFS) {
+        using App = apps::BFS<uint32_t, uint32_t, graphs::NoWeight>;
+        const bool non_atomic = o.non_atomic != 0;
+        auto qs = build([non_atomic](uint32_t s) { return App(s, non_atomic); }, (App *)nullptr);
+        return run.template go<App, uint32_t, uint32_t, graphs::NoWeight>(qs, graphs, outs, p);
+    }
+    if (algo == SG_QUERY_BC) {
+        // HybridBC forces FINE_GRAINED load balancing (hybrid_bc.cu:335-336)
+        if (o.lb_push < 0) p.lb_push = engine::LB_FINE;
+        if (o.lb_pull < 0) p.lb_pull = engine::LB_FINE;
+        // team state (path counts, level stack) is bound on the device
+        auto qs = build([](uint32_t s) { return BCApp(s, nullptr, nullptr, apps::LevelStack{}); }, (BCApp *)nullptr);
+        return run.template go<BCApp, uint32_t, uint32_t, graphs::NoWeight>(qs, graphs, outs, p);
+    }
+    return SG_ERR_INVALID_ARG;
+}
+
+struct DirectRun {
+    sg_ctx *ctx;
+    const sg_options &o;
+    sg_stats *stats;
+    float *per_query_ms;
+    template <typename App, typename TV, typename TB, typename TW>
+    sg_status go(std::vector<engine::BatchQuery<App, TV>> &qs, const std::vector<sg_graph *> &graphs,
+                 const std::vector<void *> &outs, engine::Params p) {
+        return run_batch<App, TV, TB, TW>(ctx, std::move(qs), graphs, outs, o, p, stats, per_query_ms);
+    }
+};
+
+sg_status batch_entry(int algo, sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt,
+                      sg_stats *stats, float *per_query_ms) {
+    sg_status st = check_batch(ctx, q, n);
+    if (st != SG_OK) return st;
+    DevGuard dg(ctx->device);
+    sg_options o;
+    if (opt)
+        o = *opt;
+    else
+        sg_options_default(&o);
+    DirectRun run{ctx, o, stats, per_query_ms};
+    return dispatch_batch(algo, q, n, o, run);
+}
+
 }  // namespace
 
 extern "C" sg_status sg_sssp_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt,
                                    sg_stats *stats, float *per_query_ms) {
-    sg_status st = check_batch(ctx, q, n);
-    if (st != SG_OK) return st;
-    DevGuard dg(ctx->device);
-    sg_options o;
-    if (opt)
-        o = *opt;
-    else
-        sg_options_default(&o);
-    engine::Params p = batch_params(o, 0);
-    using App = apps::SSSP<uint32_t, uint32_t, uint32_t>;
-    std::vector<engine::BatchQuery<App, uint32_t>> qs;
-    qs.reserve(n);
-    std::vector<sg_graph *> graphs(n);
-    std::vector<void *> outs(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        App app(q[i].source);
-        qs.push_back(make_query(app, q[i].graph));
-        graphs[i] = q[i].graph;
-        outs[i] = q[i].out;
-        if (!q[i].graph->has_csc && p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
-    }
-    if (o.priority == SG_PRIORITY_LOW_HIGH) {
-        // one delta for the batch: the reference heuristic on the largest graph unless given
-        double delta = o.priority_delta;
-        if (delta <= 0) {
-            const sg_graph *g = *std::max_element(graphs.begin(), graphs.end(),
-                                                  [](const sg_graph *a, const sg_graph *b) { return a->ne < b->ne; });
-            delta = std::max(1.0, std::floor(32.0 * (g->ne ? g->weight_sum / g->ne : 1.0) / ((double)g->ne / g->nv)));
-        }
-        p.priority = 1;
-        p.prio_init_raw = p.prio_step_raw = engine::to_raw<uint32_t>((uint32_t)delta);
-        if (p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
-        p.collect = 0;
-    }
-    return run_batch<App, uint32_t, uint32_t, uint32_t>(ctx, qs, graphs, outs, o, p, stats, per_query_ms);
+    return batch_entry(SG_QUERY_SSSP, ctx, q, n, opt, stats, per_query_ms);
 }
 
 extern "C" sg_status sg_bfs_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt,
                                   sg_stats *stats, float *per_query_ms) {
-    sg_status st = check_batch(ctx, q, n);
-    if (st != SG_OK) return st;
-    DevGuard dg(ctx->device);
-    sg_options o;
-    if (opt)
-        o = *opt;
-    else
-        sg_options_default(&o);
-    engine::Params p = batch_params(o, 0);
-    using App = apps::BFS<uint32_t, uint32_t, graphs::NoWeight>;
-    std::vector<engine::BatchQuery<App, uint32_t>> qs;
-    qs.reserve(n);
-    std::vector<sg_graph *> graphs(n);
-    std::vector<void *> outs(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        App app(q[i].source, o.non_atomic != 0);
-        qs.push_back(make_query(app, q[i].graph));
-        graphs[i] = q[i].graph;
-        outs[i] = q[i].out;
-        if (!q[i].graph->has_csc && p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
-    }
-    return run_batch<App, uint32_t, uint32_t, graphs::NoWeight>(ctx, qs, graphs, outs, o, p, stats, per_query_ms);
+    return batch_entry(SG_QUERY_BFS, ctx, q, n, opt, stats, per_query_ms);
 }
 
 extern "C" sg_status sg_bc_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t n, const sg_options *opt,
                                  sg_stats *stats, float *per_query_ms) {
+    return batch_entry(SG_QUERY_BC, ctx, q, n, opt, stats, per_query_ms);
+}
+
+// ---------------------------------------------------------------- planned batches (CUDA graphs)
+struct sg_batch_plan {
+    sg_ctx *ctx = nullptr;
+    sgb::Workspace ws;  // owned: a captured graph holds these addresses
+    BatchBuild B;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool captured = false;
+    bool launched = false;
+};
+
+namespace {
+
+struct PlanRun {
+    sg_batch_plan *plan;
+    const sg_options &o;
+    template <typename App, typename TV, typename TB, typename TW>
+    sg_status go(std::vector<engine::BatchQuery<App, TV>> &qs, const std::vector<sg_graph *> &graphs,
+                 const std::vector<void *> &outs, engine::Params p) {
+        return prepare_batch<App, TV, TB, TW>(plan->ctx, plan->ws, std::move(qs), graphs, outs, o, p, true, plan->B);
+    }
+};
+
+}  // namespace
+
+extern "C" sg_status sg_batch_plan_create(sg_ctx *ctx, int algo, const sg_batch_query *q, uint32_t n,
+                                          const sg_options *opt, sg_batch_plan **out) {
+    if (!out || (algo != SG_QUERY_BFS && algo != SG_QUERY_SSSP && algo != SG_QUERY_BC)) return SG_ERR_INVALID_ARG;
+    *out = nullptr;
     sg_status st = check_batch(ctx, q, n);
     if (st != SG_OK) return st;
     DevGuard dg(ctx->device);
@@ -875,20 +1015,62 @@ extern "C" sg_status sg_bc_batch(sg_ctx *ctx, const sg_batch_query *q, uint32_t 
         o = *opt;
     else
         sg_options_default(&o);
-    engine::Params p = batch_params(o, 0);
-    // HybridBC forces FINE_GRAINED load balancing (hybrid_bc.cu:335-336)
-    if (o.lb_push < 0) p.lb_push = engine::LB_FINE;
-    if (o.lb_pull < 0) p.lb_pull = engine::LB_FINE;
-    std::vector<engine::BatchQuery<BCApp, uint32_t>> qs;
-    qs.reserve(n);
-    std::vector<sg_graph *> graphs(n);
-    std::vector<void *> outs(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        BCApp app(q[i].source, nullptr, nullptr, apps::LevelStack{});  // team state is bound on the device
-        qs.push_back(make_query(app, q[i].graph));
-        graphs[i] = q[i].graph;
-        outs[i] = q[i].out;
-        if (!q[i].graph->has_csc && p.forced < 0) p.forced = engine::V_ASYNC_PUSH_DD;
+    auto plan = std::make_unique<sg_batch_plan>();
+    plan->ctx = ctx;
+    PlanRun run{plan.get(), o};
+    if ((st = dispatch_batch(algo, q, n, o, run)) != SG_OK) return st;
+    SG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // descriptors are on the device
+    // Capture memsets + the cooperative launch once; a driver that cannot
+    // capture them leaves the plan on direct launches (same work, more calls).
+    cudaStream_t s = ctx->stream;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const sg_status est = enqueue_batch(ctx, plan->B, s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s, &g);
+        if (est == SG_OK && ce == cudaSuccess && g &&
+            cudaGraphInstantiate(&plan->exec, g, 0) == cudaSuccess) {
+            plan->graph = g;
+            plan->captured = true;
+        } else if (g) {
+            cudaGraphDestroy(g);
+        }
     }
-    return run_batch<BCApp, uint32_t, uint32_t, graphs::NoWeight>(ctx, qs, graphs, outs, o, p, stats, per_query_ms);
+    cudaGetLastError();  // a refused capture leaves no error behind
+    ctx->last_error.clear();
+    *out = plan.release();
+    return SG_OK;
+}
+
+extern "C" sg_status sg_batch_plan_launch(sg_batch_plan *plan) {
+    if (!plan) return SG_ERR_INVALID_ARG;
+    sg_ctx *ctx = plan->ctx;
+    DevGuard dg(ctx->device);
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    if (plan->captured) {
+        SG_TRY_CUDA(ctx, cudaGraphLaunch(plan->exec, ctx->stream));
+    } else {
+        const sg_status st = enqueue_batch(ctx, plan->B, ctx->stream);
+        if (st != SG_OK) return st;
+    }
+    SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    plan->launched = true;
+    return SG_OK;
+}
+
+extern "C" sg_status sg_batch_plan_wait(sg_batch_plan *plan, sg_stats *stats, float *per_query_ms) {
+    if (!plan || !plan->launched) return SG_ERR_INVALID_ARG;
+    DevGuard dg(plan->ctx->device);
+    return finish_batch(plan->ctx, plan->ws, plan->B, false, stats, per_query_ms);
+}
+
+extern "C" int sg_batch_plan_captured(const sg_batch_plan *plan) { return plan && plan->captured ? 1 : 0; }
+
+extern "C" sg_status sg_batch_plan_destroy(sg_batch_plan *plan) {
+    if (!plan) return SG_ERR_INVALID_ARG;
+    DevGuard dg(plan->ctx->device);
+    cudaStreamSynchronize(plan->ctx->stream);
+    if (plan->exec) cudaGraphExecDestroy(plan->exec);
+    if (plan->graph) cudaGraphDestroy(plan->graph);
+    delete plan;
+    return SG_OK;
 }

@@ -77,7 +77,8 @@ struct alignas(16) RoundState {
     uint32_t round, done;
     uint32_t qin, qhi, qlo, bin;
     uint32_t bout, dirty, pile, F;
-    uint32_t heavy_expected, pad;
+    uint32_t heavy_expected;  // heavy vertices forecast for this round (level-synchronous apps)
+    uint32_t chunks;          // chunks registered by the previous push round, run at this round's start
     unsigned long long prio_raw;
 };
 static_assert(sizeof(RoundState) == 64, "snapshot is four 16-byte loads");
@@ -87,7 +88,8 @@ struct Counters {
     uint32_t qcount[4];
     uint32_t heavy_enq[4];
     unsigned long long scout[4];
-    uint32_t middle_count, heavy_count, chunk_count, error;
+    uint32_t middle_count, error;
+    uint32_t heavy_count[2], chunk_count[2];  // heavy-vertex tables, one set per round parity
     unsigned long long edges_processed;
 };
 
@@ -135,9 +137,9 @@ struct KArgs {
     uint32_t *qflag[3];  // queued bitmap of each worklist slot
     uint32_t nwords;
     uint32_t *middle;
-    HeavyItem<TBuffer> *heavy;
+    HeavyItem<TBuffer> *heavy;  // 2 * heavy_cap items: set k starts at heavy + k * heavy_cap
     uint32_t heavy_cap;
-    uint32_t *chunk_owner;
+    uint32_t *chunk_owner;      // 2 * chunk_cap entries, likewise
     uint32_t chunk_cap;
     Ctrl *ctrl;
     sg_round_trace *trace;
@@ -211,6 +213,20 @@ struct has_pull_reduce<App, TB,
                        std::void_t<decltype(std::declval<const App &>().PullReduce(std::declval<TB>(),
                                                                                     std::declval<TB>()))>>
     : std::true_type {};
+
+// Functors whose result does not depend on the order in which pushes are
+// applied (monotone label correction as in BFS/SSSP, residual accumulation as
+// in PageRank) declare `static constexpr bool kReorderSafe = true`.  For them,
+// when every round is ASYNC_PUSH_DD (a forced variant), the chunks of heavy
+// vertices found in a round run at the start of the next round instead of
+// behind an extra barrier.  Under the hybrid policy the next round may be a
+// pull round, whose frontier must already hold every vertex those chunks would
+// reach, and level-synchronous functors (BC's path counting) need both halves
+// of a round apart, so both keep the barrier.
+template <typename App, typename = void>
+struct reorder_safe : std::false_type {};
+template <typename App>
+struct reorder_safe<App, std::void_t<decltype(App::kReorderSafe)>> : std::integral_constant<bool, App::kReorderSafe> {};
 
 // Dispatch to the weighted or unweighted AccumulateBuffer overload like
 // PushFunctor/PullFunctor do (push_functor.h:123-138).  Unweighted graphs
@@ -381,8 +397,8 @@ struct EngineKernel {
 
     // Registers the lanes' heavy vertices as chunk lists (warp-aggregated: one
     // ballot, one scan, two atomics per warp).  All 32 lanes must call.
-    static __device__ __forceinline__ void register_heavy(const Args &a, bool heavy, uint32_t src, uint32_t beg,
-                                                          uint32_t deg, TB payload) {
+    static __device__ __forceinline__ void register_heavy(const Args &a, uint32_t set, bool heavy, uint32_t src,
+                                                          uint32_t beg, uint32_t deg, TB payload) {
         const uint32_t m = __ballot_sync(dev::kFullMask, heavy);
         if (m == 0) return;
         Counters *n = &a.ctrl->cnt;
@@ -394,8 +410,8 @@ struct EngineKernel {
         const uint32_t leader = __ffs(m) - 1;
         uint32_t hb = 0, cb = 0;
         if (lane == leader) {
-            hb = atomicAdd(&n->heavy_count, (uint32_t)__popc(m));
-            cb = atomicAdd(&n->chunk_count, tot);
+            hb = atomicAdd(&n->heavy_count[set], (uint32_t)__popc(m));
+            cb = atomicAdd(&n->chunk_count[set], tot);
         }
         hb = __shfl_sync(dev::kFullMask, hb, leader);
         cb = __shfl_sync(dev::kFullMask, cb, leader);
@@ -409,8 +425,9 @@ struct EngineKernel {
             h.deg = deg;
             h.chunk_base = c0;
             h.payload = payload;
-            a.heavy[idx] = h;
-            for (uint32_t i = 0; i < nch; ++i) a.chunk_owner[c0 + i] = idx;
+            a.heavy[(size_t)set * a.heavy_cap + idx] = h;
+            uint32_t *own = a.chunk_owner + (size_t)set * a.chunk_cap;
+            for (uint32_t i = 0; i < nch; ++i) own[c0 + i] = idx;
         } else {
             atomicOr(&n->error, dev::kErrChunkCapacity);
         }
@@ -513,16 +530,18 @@ struct EngineKernel {
         acc.edges += e - beg;
     }
 
-    // Chunks of heavy vertices registered in phase A, spread over all warps.
-    static __device__ void heavy_phase(App &app, const Args &a, const Snap &s, bool dd, Acc &acc) {
-        const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count), a.chunk_cap);
-        const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count), a.heavy_cap);
+    // Chunks of the heavy vertices registered in table `set`, spread over all warps.
+    static __device__ void heavy_phase(App &app, const Args &a, const Snap &s, uint32_t set, bool dd, Acc &acc) {
+        const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count[set]), a.chunk_cap);
+        const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count[set]), a.heavy_cap);
+        const uint32_t *own = a.chunk_owner + (size_t)set * a.chunk_cap;
+        const HeavyItem<TB> *items = a.heavy + (size_t)set * a.heavy_cap;
         const uint32_t lane = dev::lane_id();
         const uint32_t ce = a.p.chunk_edges;
         for (uint32_t ch = gwarp(); ch < C; ch += nwarps()) {
-            const uint32_t e = dev::ld_l2(a.chunk_owner + ch);
+            const uint32_t e = dev::ld_l2(own + ch);
             if (e >= H) continue;
-            const HeavyItem<TB> h = a.heavy[e];
+            const HeavyItem<TB> h = items[e];
             if (ch < h.chunk_base) continue;
             const uint32_t off = (ch - h.chunk_base) * ce;
             if (off >= h.deg) continue;
@@ -621,7 +640,7 @@ struct EngineKernel {
                 continue;
             }
             const bool heavy = deg > a.p.heavy_threshold;
-            register_heavy(a, heavy, v, beg, deg, payload);
+            register_heavy(a, s.round & 1u, heavy, v, beg, deg, payload);
             if (heavy) deg = 0;
             expand_warp(app, a, s, wlb, v, beg, deg, payload, dd, acc);
         }
@@ -756,7 +775,7 @@ struct EngineKernel {
                     deg = a.csc.end_edge(v) - beg;
                 }
                 const bool heavy = deg > a.p.heavy_threshold;
-                register_heavy(a, heavy, v, beg, deg, app.PullIdentity());
+                register_heavy(a, s.round & 1u, heavy, v, beg, deg, app.PullIdentity());
                 if (heavy) deg = 0;
                 const uint32_t incl = dev::warp_inclusive_scan(deg);
                 const uint32_t total = __shfl_sync(dev::kFullMask, incl, 31);
@@ -791,16 +810,18 @@ struct EngineKernel {
         }
     }
 
-    static __device__ void pull_reduce_chunks(App &app, const Args &a, Acc &acc) {
+    static __device__ void pull_reduce_chunks(App &app, const Args &a, uint32_t set, Acc &acc) {
         if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value) {
-            const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count), a.chunk_cap);
-            const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count), a.heavy_cap);
+            const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count[set]), a.chunk_cap);
+            const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count[set]), a.heavy_cap);
+            const uint32_t *own = a.chunk_owner + (size_t)set * a.chunk_cap;
+            const HeavyItem<TB> *items = a.heavy + (size_t)set * a.heavy_cap;
             const uint32_t lane = dev::lane_id();
             const uint32_t ce = a.p.chunk_edges;
             for (uint32_t ch = gwarp(); ch < C; ch += nwarps()) {
-                const uint32_t e = dev::ld_l2(a.chunk_owner + ch);
+                const uint32_t e = dev::ld_l2(own + ch);
                 if (e >= H) continue;
-                const HeavyItem<TB> h = a.heavy[e];
+                const HeavyItem<TB> h = items[e];
                 if (ch < h.chunk_base) continue;
                 const uint32_t off = (ch - h.chunk_base) * ce;
                 if (off >= h.deg) continue;
@@ -834,6 +855,11 @@ struct EngineKernel {
     }
 
     // ---------------------------------------------------------------- leader (block 0, thread 0)
+    // Heavy-vertex chunks of a round run at the start of the next one (see reorder_safe).
+    static __device__ __forceinline__ bool defer_chunks(const Args &a) {
+        return reorder_safe<App>::value && a.p.forced == V_ASYNC_PUSH_DD && a.p.lb_push != LB_NONE;
+    }
+
     static __device__ bool supported(const Args &a, int v) {
         if (v == V_SYNC_PUSH_TD || v == V_SYNC_PUSH_DD || v == V_ASYNC_PULL_TD) return false;
         if (is_pull(v) && !a.p.has_csc) return false;
@@ -942,6 +968,10 @@ struct EngineKernel {
             sc[k] = dev::ld_l2(&n->scout[k]);
         }
         const uint32_t err = dev::ld_l2(&n->error);
+        // chunks of this round's heavy vertices left for the next round's start
+        const uint32_t cur = rs.round & 1u;
+        const bool deferred = defer_chunks(a);
+        const uint32_t pend = deferred ? min(dev::ld_l2(&n->chunk_count[cur]), a.chunk_cap) : 0u;
         app.App::PostComputation();
         ps.rounds_by_variant[var & 7]++;
         const unsigned long long now = dev::globaltimer_ns();
@@ -976,15 +1006,16 @@ struct EngineKernel {
         if (a.p.forced < 0) next = a.p.scheme == 0 ? traversal_policy(a, ps, var) : iterative_policy(ps, var);
         const bool fatal = (err & (dev::kErrTimeout | dev::kErrCapacity | dev::kErrChunkCapacity |
                                    dev::kErrUnsupported | dev::kErrOverflow)) != 0;
-        if (ps.output_active == 0 || rs.round >= a.p.max_iteration || fatal) {
-            ps.max_iteration_reached = ps.output_active != 0 && rs.round >= a.p.max_iteration;
+        const bool work_left = ps.output_active != 0 || pend != 0;
+        if (!work_left || rs.round >= a.p.max_iteration || fatal) {
+            ps.max_iteration_reached = work_left && rs.round >= a.p.max_iteration;
             finish(a, ps, now);
             publish(a, ps);
             return;
         }
         // rotate worklists
         uint32_t reset_q;
-        if (prio_push && out_hi == 0) {
+        if (prio_push && out_hi == 0 && pend == 0) {
             // near pile drained: open the next priority window over the far pile (driver.cuh:668-675)
             rs.prio_raw = to_raw<TB>((TB)(from_raw<TB>(rs.prio_raw) + from_raw<TB>(a.p.prio_step_raw)));
             const uint32_t t = rs.qin;
@@ -1021,9 +1052,16 @@ struct EngineKernel {
         rs.round++;
         rs.F = min(qc[rs.qin], a.queue_cap);
         rs.heavy_expected = a.p.collect ? he[rs.qin] : (rs.F > 0);
+        rs.chunks = pend;
         n->middle_count = 0;
-        n->heavy_count = 0;
-        n->chunk_count = 0;
+        // the previous round's deferred set ran at the start of this round; this
+        // round's set either ran inside the round or is now pending
+        n->heavy_count[cur ^ 1u] = 0;
+        n->chunk_count[cur ^ 1u] = 0;
+        if (!pend) {
+            n->heavy_count[cur] = 0;
+            n->chunk_count[cur] = 0;
+        }
         pre_bookkeeping(a, ps, rs.F, sc[rs.qin]);
         publish(a, ps);
         ps.t_round_start = dev::globaltimer_ns();
@@ -1084,15 +1122,24 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         K::load_snap(a, s);
         if (s.done) break;
         const int var = s.variant;
+        const uint32_t set = s.round & 1u;  // heavy-vertex table this round registers into
         K::set_app_variant(app, var);
+        if (s.chunks) {
+            // chunks of the heavy vertices the previous push round found (reorder-safe functors only)
+            K::heavy_phase(app, a, s, set ^ 1u, true, acc);
+            if (var != V_ASYNC_PUSH_DD) {  // not reached while chunks are deferred only under forced push DD
+                K::flush_acc(a, acc, s.qhi, s.qlo);
+                if (!grid_sync(c, tmo, nop)) return false;
+            }
+        }
         switch (var) {
             case V_ASYNC_PUSH_DD: {
                 K::clear_dirty(a, s);
                 K::push_phase_a(app, a, s, my_lb, true, lb_push, acc);
-                if (s.heavy_expected > 0 && lb_push != LB_NONE) {
+                if (!K::defer_chunks(a) && s.heavy_expected > 0 && lb_push != LB_NONE) {
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                     if (!grid_sync(c, tmo, nop)) return false;
-                    K::heavy_phase(app, a, s, true, acc);
+                    K::heavy_phase(app, a, s, set, true, acc);
                 }
                 K::flush_acc(a, acc, s.qhi, s.qlo);
                 break;
@@ -1104,7 +1151,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
                 K::flush_acc(a, acc, s.qhi, s.qlo);
                 if (!grid_sync(c, tmo, nop)) return false;
                 if (lb_push != LB_NONE) {
-                    K::heavy_phase(app, a, s, false, acc);
+                    K::heavy_phase(app, a, s, set, false, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                     if (!grid_sync(c, tmo, nop)) return false;
                 }
@@ -1127,7 +1174,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
                     K::pull_reduce_td(app, a, s, my_lb, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                     if (!grid_sync(c, tmo, nop)) return false;
-                    K::pull_reduce_chunks(app, a, acc);
+                    K::pull_reduce_chunks(app, a, set, acc);
                 } else {
                     K::pull_phase(app, a, s, dd, sync, lb_pull, acc);
                 }
@@ -1167,6 +1214,7 @@ struct BatchQuery {
     graphs::dev::CSCGraph csc;
     const uint32_t *csr_w, *csc_w;
     TV *value;
+    unsigned long long prio_raw;  // this query's two-level priority step (0 = the batch's)
 };
 
 // Per-team workspace of a batched launch, sized for the largest graph of the
@@ -1257,6 +1305,7 @@ __global__ void __launch_bounds__(kBlockThreads)
         a.trace_cap = 0;
         a.p = p;
         a.p.total_workload0 = (long long)bq.csr.nedges;
+        if (bq.prio_raw) a.p.prio_init_raw = a.p.prio_step_raw = bq.prio_raw;
         App app = bq.app;
         app.m_p_current_round = &c->rs.round;
         if (!run_instance<App, TV, TB, TW>(app, a)) return;

@@ -15,5 +15,7 @@ sg_status msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint32_t n
 
 // The context a graph was created on.
 sg_ctx *graph_context(const sg_graph *g);
+// Sum of the graph's edge weights (its edge count when unweighted).
+double graph_weight_sum(const sg_graph *g);
 
 }  // namespace sgb

@@ -6,7 +6,7 @@
 // paths that must not allocate while the device is being shared.  For them
 // this entry point runs the same hybrid BFS engine as sg_bfs, but every
 // worklist, bitmap and control word lives in one file-scope device array of
-// fixed size (kNoAllocScratchBytes, about 13 MB), so the call allocates
+// fixed size (kNoAllocScratchBytes, about 19 MB), so the call allocates
 // nothing.  The caller passes the graph (device CSR, optionally the device
 // in-edge CSC) and the device output array.
 //
@@ -54,8 +54,9 @@ constexpr size_t kOffMiddle = kOffQueue + 3 * align256(4ull * kNoAllocMaxVertice
 constexpr size_t kOffBitmap = kOffMiddle + align256(4ull * kNoAllocMaxVertices);
 constexpr size_t kOffFlag = kOffBitmap + 2 * align256(4ull * kWords);
 constexpr size_t kOffHeavy = kOffFlag + 3 * align256(4ull * kWords);
-constexpr size_t kOffChunk = kOffHeavy + align256(sizeof(HeavyItem<uint32_t>) * kHeavyCap);
-constexpr size_t kOffCtrl = kOffChunk + align256(4ull * kChunkCap);
+// two heavy-vertex tables and two chunk tables (one per round parity)
+constexpr size_t kOffChunk = kOffHeavy + align256(2 * sizeof(HeavyItem<uint32_t>) * kHeavyCap);
+constexpr size_t kOffCtrl = kOffChunk + align256(2 * 4ull * kChunkCap);
 constexpr size_t kNoAllocScratchBytes = kOffCtrl + align256(sizeof(Ctrl));
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];

@@ -220,7 +220,9 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     // A warp task is 32 light vertices (<= heavy_threshold edges each) or one
     // chunk of a heavy vertex (<= chunk_edges), which bounds the slowest warp
     // of a round.  Each vertex is registered at most once per round, so the
-    // tables are bounded by the vertices above the threshold.
+    // tables are bounded by the vertices above the threshold; there are two
+    // tables, one per round parity (a push round's chunks may run at the start
+    // of the next round while that round registers its own).
     const uint32_t heavy_threshold = std::max<uint32_t>(1, cfg.heavy_degree);
     const uint32_t chunk_edges = std::max<uint32_t>(32, cfg.chunk_edges);
     const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(nv, ne / heavy_threshold) + 2;
@@ -236,8 +238,8 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     SG_TRY_CUDA(ctx, ws.get("fl1", nwords, &a.qflag[1]));
     SG_TRY_CUDA(ctx, ws.get("fl2", nwords, &a.qflag[2]));
     SG_TRY_CUDA(ctx, ws.get("middle", nv, &a.middle));
-    SG_TRY_CUDA(ctx, ws.get("heavy", heavy_cap, &a.heavy, true));
-    SG_TRY_CUDA(ctx, ws.get("chunk", chunk_cap, &a.chunk_owner, true));
+    SG_TRY_CUDA(ctx, ws.get("heavy", 2ull * heavy_cap, &a.heavy, true));
+    SG_TRY_CUDA(ctx, ws.get("chunk", 2ull * chunk_cap, &a.chunk_owner, true));
     SG_TRY_CUDA(ctx, ws.get("ctrl", 1, &a.ctrl));
     if (cfg.trace && cfg.trace_cap) SG_TRY_CUDA(ctx, ws.get("trace", cfg.trace_cap, &a.trace));
     a.queue_cap = nv;

@@ -56,6 +56,27 @@ class Options(C.Structure):
     ]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("options", Options), ("ms", C.c_double), ("status", C.c_int32), ("pad", C.c_int32)]
+
+
+TUNED_FIELDS = ("variant", "blocks_per_sm", "heavy_degree", "priority", "priority_delta")
+VARIANT_NAMES = {-1: "auto", 0: "sync_push_td", 1: "sync_push_dd", 2: "sync_pull_td", 3: "sync_pull_dd",
+                 4: "async_push_td", 5: "async_push_dd", 6: "async_pull_td", 7: "async_pull_dd"}
+
+
+def options_dict(o: Options, fields=TUNED_FIELDS) -> dict:
+    d = {k: getattr(o, k) for k in fields}
+    if "variant" in d:
+        d["variant"] = VARIANT_NAMES.get(d["variant"], d["variant"])
+    if d.get("priority") == 0:
+        d.pop("priority")
+        d.pop("priority_delta", None)
+    elif "priority" in d:
+        d["priority"] = "low_high"
+    return d
+
+
 class RoundTrace(C.Structure):
     _fields_ = [
         ("round", C.c_uint32), ("variant", C.c_int32), ("in_nodes", C.c_uint32), ("out_nodes", C.c_uint32),
@@ -150,6 +171,15 @@ def load() -> C.CDLL:
                                    C.POINTER(C.c_float)]),
         "sg_bc_batch": (C.c_int, [_P, C.POINTER(BatchQuery), C.c_uint32, C.POINTER(Options), C.POINTER(Stats),
                                   C.POINTER(C.c_float)]),
+        "sg_batch_plan_create": (C.c_int, [_P, C.c_int, C.POINTER(BatchQuery), C.c_uint32, C.POINTER(Options),
+                                           C.POINTER(_P)]),
+        "sg_batch_plan_launch": (C.c_int, [_P]),
+        "sg_batch_plan_wait": (C.c_int, [_P, C.POINTER(Stats), C.POINTER(C.c_float)]),
+        "sg_batch_plan_captured": (C.c_int, [_P]),
+        "sg_batch_plan_destroy": (C.c_int, [_P]),
+        "sg_autotune": (C.c_int, [_P, C.c_int, _U32P, C.c_uint32, C.POINTER(Options), C.c_uint32,
+                                  C.POINTER(Options), C.POINTER(C.c_double), C.POINTER(TuneEntry), C.c_uint32,
+                                  C.POINTER(C.c_uint32)]),
         "sg_msbfs_on": (C.c_int, [_P, _P, _U32P, C.c_uint32, C.POINTER(Options), _P, C.POINTER(Stats)]),
         "sg_server_config_default": (C.c_int, [C.POINTER(ServerConfig)]),
         "sg_server_create": (C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_P)]),
@@ -340,6 +370,7 @@ class Context:
     def __init__(self, device: int = 0):
         self._c = _P()
         self._graphs = weakref.WeakSet()
+        self._plans = weakref.WeakSet()
         _check(load().sg_init(device, C.byref(self._c)), "sg_init")
         self.device = device
 
@@ -389,6 +420,11 @@ class Context:
     def bfs_batch(self, queries, outs=None, team_blocks: int = 0, **opts):
         return self._batch(load().sg_bfs_batch, "sg_bfs_batch", queries, outs, team_blocks, opts)
 
+    def batch_plan(self, algo: str, queries, outs, team_blocks: int = 0, **opts) -> "BatchPlan":
+        """Plans queries [(Graph, source)] of `algo` ("bfs", "sssp", "bc") once for repeated launches
+        (sg_batch_plan_*); outs are device arrays (e.g. torch CUDA tensors) of each graph's nv elements."""
+        return BatchPlan(self, algo, queries, outs, team_blocks, opts)
+
     def bc_batch(self, queries, outs=None, team_blocks: int = 0, **opts):
         """Single-source BC of every (Graph, source) in one launch; outputs are float32 arrays."""
         return self._batch(load().sg_bc_batch, "sg_bc_batch", queries, outs, team_blocks, opts, np.float32)
@@ -415,10 +451,56 @@ class Context:
     def close(self):
         """Releases the context; graphs still open on it are released first."""
         if self._c:
+            for p in list(self._plans):  # plans hold graphs and the context's stream
+                p.close()
             for g in list(self._graphs):
                 g.close()
             load().sg_destroy(self._c)
             self._c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchPlan:
+    """A batch planned once; each launch replays one CUDA graph (see sg_batch_plan_create)."""
+
+    def __init__(self, ctx, algo, queries, outs, team_blocks, opts):
+        n = len(queries)
+        arr = (BatchQuery * n)()
+        for i, ((g, s), o) in enumerate(zip(queries, outs)):
+            arr[i].graph = g.handle
+            arr[i].source = int(s)
+            arr[i].out = _ptr(o)
+        o = make_options(**opts)
+        if team_blocks:
+            o.reserved[0] = int(team_blocks)
+        self.ctx, self.n, self._outs = ctx, n, list(outs)
+        self._p = _P()
+        _check(load().sg_batch_plan_create(ctx.handle, QUERY_ALGOS[algo], arr, n, C.byref(o), C.byref(self._p)),
+               "sg_batch_plan_create", ctx.handle)
+        ctx._plans.add(self)
+
+    @property
+    def captured(self) -> bool:
+        return bool(load().sg_batch_plan_captured(self._p))
+
+    def launch(self):
+        _check(load().sg_batch_plan_launch(self._p), "sg_batch_plan_launch", self.ctx.handle)
+
+    def wait(self):
+        st = Stats()
+        per = (C.c_float * self.n)()
+        _check(load().sg_batch_plan_wait(self._p, C.byref(st), per), "sg_batch_plan_wait", self.ctx.handle)
+        return st, list(per)
+
+    def close(self):
+        if self._p:
+            load().sg_batch_plan_destroy(self._p)
+            self._p = None
 
     def __del__(self):
         try:
@@ -540,6 +622,21 @@ class Graph:
         _check(load().sg_pagerank(self._g, C.byref(o), _ptr(out), _ptr(residual_out), C.byref(st)), "sg_pagerank",
                self.ctx.handle)
         return out, st, self._trace(buf, st)
+
+    def autotune(self, algo: str, sources=(), max_candidates: int = 0, **base_opts):
+        """Times the library's candidate options for `algo` on these sources (sg_autotune).
+
+        Returns (best options as a dict of keyword arguments, best ms, report)."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        base = make_options(**base_opts)
+        best, best_ms = Options(), C.c_double()
+        rep = (TuneEntry * 64)()
+        n = C.c_uint32()
+        _check(load().sg_autotune(self._g, QUERY_ALGOS[algo], src.ctypes.data_as(_U32P), len(src), C.byref(base),
+                                  max_candidates, C.byref(best), C.byref(best_ms), rep, 64, C.byref(n)),
+               "sg_autotune", self.ctx.handle)
+        report = [dict(options_dict(rep[i].options), ms=rep[i].ms, status=rep[i].status) for i in range(n.value)]
+        return options_dict(best), best_ms.value, report
 
     def msbfs(self, sources, out=None, **opts):
         """BFS from up to 64 sources in one launch; returns (levels[nsrc, nv], stats)."""

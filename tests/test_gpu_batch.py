@@ -135,3 +135,40 @@ def test_bc_batch_matches_single_and_oracle(ctx, team_blocks):
         if h.nv <= 1024:
             want, _, _ = oracle.bc_f64(h.offsets, h.indices, s)
             assert np.allclose(o, want, rtol=1e-4, atol=1e-4), s
+
+
+@pytest.mark.parametrize("algo", ["sssp", "bfs", "bc"])
+def test_batch_plan_replays_match_direct_batch(ctx, uneven_graphs, algo):
+    """A planned batch launched three times gives the direct batch's outputs every time."""
+    torch = pytest.importorskip("torch")
+    queries = [(G, int(h.pick_sources(1, 70 + k)[0])) for k, (h, G) in enumerate(uneven_graphs)] * 2
+    kw = dict(max_iteration=100000)
+    if algo == "sssp":
+        want, _, _ = ctx.sssp_batch(queries, **kw)
+    elif algo == "bfs":
+        want, _, _ = ctx.bfs_batch(queries, **kw)
+    else:
+        want, _, _ = ctx.bc_batch(queries, **kw)
+    dt = torch.float32 if algo == "bc" else torch.int32
+    outs = [torch.zeros(G.nv, dtype=dt, device="cuda") for G, _ in queries]
+    plan = ctx.batch_plan(algo, queries, outs, **kw)
+    for rep in range(3):
+        for o in outs:
+            o.zero_()
+        torch.cuda.synchronize()  # the zeroing (torch's stream) precedes the plan's launch (the context's stream)
+        plan.launch()
+        st, per = plan.wait()
+        assert st.device_error == 0 and len(per) == len(queries)
+        for o, w in zip(outs, want):
+            got = o.cpu().numpy()
+            if algo == "bc":
+                assert np.allclose(got, w, rtol=1e-4, atol=1e-5), rep
+            else:
+                assert (got.view(np.uint32) == w).all(), rep
+    plan.close()
+
+
+def test_batch_plan_rejects_host_outputs(ctx, uneven_graphs):
+    h, G = uneven_graphs[0]
+    with pytest.raises(sg.SGError):
+        ctx.batch_plan("bfs", [(G, 0)], [np.zeros(h.nv, np.uint32)])
