@@ -23,7 +23,6 @@ constexpr uint32_t kInf = 0xffffffffu;  // IDENTITY_ELEMENT of BFS/SSSP/BC (UINT
 template <typename TValue, typename TBuffer, typename TWeight, typename... Unused>
 struct BFS : AppBase<TValue, TBuffer, TWeight> {
     using AppBase<TValue, TBuffer, TWeight>::AccumulateBuffer;
-    static constexpr bool kReorderSafe = true;  // result independent of push order
     index_t m_source_node;
     bool m_non_atomic;
 
@@ -68,6 +67,10 @@ struct BFS : AppBase<TValue, TBuffer, TWeight> {
     }
 
     __forceinline__ __device__ bool IsActiveNode(index_t, TBuffer buffer) const override { return buffer != kInf; }
+    // Levels are a monotone minimum only when the accumulation is atomic: a
+    // plain store may overwrite a smaller level pushed concurrently by a round
+    // of another depth (all pushes of one BFS round carry the same level).
+    __forceinline__ __device__ bool ReorderSafe() const { return !m_non_atomic; }
 };
 
 // ---------------------------------------------------------------- SSSP
@@ -78,7 +81,6 @@ struct BFS : AppBase<TValue, TBuffer, TWeight> {
 template <typename TValue, typename TBuffer, typename TWeight, typename... Unused>
 struct SSSP : AppBase<TValue, TBuffer, TWeight> {
     using AppBase<TValue, TBuffer, TWeight>::AccumulateBuffer;
-    static constexpr bool kReorderSafe = true;  // result independent of push order
     index_t m_source_node;
 
     explicit SSSP(index_t source) : m_source_node(source) {}
@@ -111,6 +113,7 @@ struct SSSP : AppBase<TValue, TBuffer, TWeight> {
     __forceinline__ __device__ bool IsHighPriority(TBuffer current_priority, TBuffer buffer) const override {
         return current_priority > buffer;
     }
+    __forceinline__ __device__ bool ReorderSafe() const { return true; }  // atomic monotone minimum
 };
 
 // ---------------------------------------------------------------- PageRank
@@ -122,7 +125,6 @@ struct SSSP : AppBase<TValue, TBuffer, TWeight> {
 template <typename TValue, typename TBuffer, typename TWeight, typename... Unused>
 struct PageRank : AppBase<TValue, TBuffer, TWeight> {
     using AppBase<TValue, TBuffer, TWeight>::AccumulateBuffer;
-    static constexpr bool kReorderSafe = true;  // result independent of push order
     double m_error;
 
     explicit PageRank(double error) : m_error(error) {}
@@ -157,6 +159,8 @@ struct PageRank : AppBase<TValue, TBuffer, TWeight> {
 
     __forceinline__ __device__ TBuffer PullReduce(TBuffer a, TBuffer b) const { return a + b; }
     __forceinline__ __device__ TBuffer PullIdentity() const { return (TBuffer)0.0f; }
+    // residual pushes are atomic additions: any order reaches the same fixed point within the threshold
+    __forceinline__ __device__ bool ReorderSafe() const { return true; }
 };
 
 // ---------------------------------------------------------------- BC

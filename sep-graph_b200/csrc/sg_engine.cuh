@@ -215,8 +215,10 @@ struct has_pull_reduce<App, TB,
     : std::true_type {};
 
 // Functors whose result does not depend on the order in which pushes are
-// applied (monotone label correction as in BFS/SSSP, residual accumulation as
-// in PageRank) declare `static constexpr bool kReorderSafe = true`.  For them,
+// applied (atomic monotone label correction as in BFS/SSSP, residual
+// accumulation as in PageRank) declare `bool ReorderSafe() const` returning
+// true (BFS only when its accumulation is atomic: a plain store may lose a
+// smaller level written concurrently by a push of another level).  For them,
 // when every round is ASYNC_PUSH_DD (a forced variant), the chunks of heavy
 // vertices found in a round run at the start of the next round instead of
 // behind an extra barrier.  Under the hybrid policy the next round may be a
@@ -224,9 +226,16 @@ struct has_pull_reduce<App, TB,
 // reach, and level-synchronous functors (BC's path counting) need both halves
 // of a round apart, so both keep the barrier.
 template <typename App, typename = void>
-struct reorder_safe : std::false_type {};
+struct has_reorder_safe : std::false_type {};
 template <typename App>
-struct reorder_safe<App, std::void_t<decltype(App::kReorderSafe)>> : std::integral_constant<bool, App::kReorderSafe> {};
+struct has_reorder_safe<App, std::void_t<decltype(std::declval<const App &>().ReorderSafe())>> : std::true_type {};
+template <typename App>
+__device__ __forceinline__ bool reorder_safe(const App &app) {
+    if constexpr (has_reorder_safe<App>::value)
+        return app.ReorderSafe();
+    else
+        return false;
+}
 
 // Dispatch to the weighted or unweighted AccumulateBuffer overload like
 // PushFunctor/PullFunctor do (push_functor.h:123-138).  Unweighted graphs
@@ -623,6 +632,13 @@ struct EngineKernel {
                 dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, keep, v, &n->error);
                 if (keep) count_enq(a, acc, false, v);
             }
+            // the row offsets are read-only: load them alongside the combine's
+            // loads instead of after it (one dependent memory trip less per round)
+            uint32_t beg = 0, end = 0;
+            if (proceed) {
+                beg = a.csr.begin_edge(v);
+                end = a.csr.end_edge(v);
+            }
             TB payload{};
             bool sched = false;
             if (proceed) {
@@ -630,11 +646,7 @@ struct EngineKernel {
                 payload = pr.first;
                 sched = pr.second;
             }
-            uint32_t beg = 0, deg = 0;
-            if (sched) {
-                beg = a.csr.begin_edge(v);
-                deg = a.csr.end_edge(v) - beg;
-            }
+            uint32_t deg = sched ? end - beg : 0u;
             if (lb == LB_NONE) {
                 if (deg) expand_serial(app, a, s, v, beg, deg, payload, dd, acc);
                 continue;
@@ -856,8 +868,8 @@ struct EngineKernel {
 
     // ---------------------------------------------------------------- leader (block 0, thread 0)
     // Heavy-vertex chunks of a round run at the start of the next one (see reorder_safe).
-    static __device__ __forceinline__ bool defer_chunks(const Args &a) {
-        return reorder_safe<App>::value && a.p.forced == V_ASYNC_PUSH_DD && a.p.lb_push != LB_NONE;
+    static __device__ __forceinline__ bool defer_chunks(const App &app, const Args &a) {
+        return a.p.forced == V_ASYNC_PUSH_DD && a.p.lb_push != LB_NONE && reorder_safe(app);
     }
 
     static __device__ bool supported(const Args &a, int v) {
@@ -970,7 +982,7 @@ struct EngineKernel {
         const uint32_t err = dev::ld_l2(&n->error);
         // chunks of this round's heavy vertices left for the next round's start
         const uint32_t cur = rs.round & 1u;
-        const bool deferred = defer_chunks(a);
+        const bool deferred = defer_chunks(app, a);
         const uint32_t pend = deferred ? min(dev::ld_l2(&n->chunk_count[cur]), a.chunk_cap) : 0u;
         app.App::PostComputation();
         ps.rounds_by_variant[var & 7]++;
@@ -1136,7 +1148,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
             case V_ASYNC_PUSH_DD: {
                 K::clear_dirty(a, s);
                 K::push_phase_a(app, a, s, my_lb, true, lb_push, acc);
-                if (!K::defer_chunks(a) && s.heavy_expected > 0 && lb_push != LB_NONE) {
+                if (!K::defer_chunks(app, a) && s.heavy_expected > 0 && lb_push != LB_NONE) {
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                     if (!grid_sync(c, tmo, nop)) return false;
                     K::heavy_phase(app, a, s, set, true, acc);
