@@ -274,27 +274,15 @@ def run_ours(a):
     G = ctx.graph(h)
     dout = torch.empty(nv, dtype=torch.int32, device="cuda")
 
-    # ---- mode selection (the project's autotuner over variant and delta), untimed
-    modes = {"hybrid": dict(max_iteration=100000), "push_dd": dict(variant="async_push_dd", max_iteration=100000)}
-    avg_w = float(h.weights.mean())
-    base_delta = max(1, int(32 * avg_w / (ne / nv)))
-    for div in (16, 8, 4, 2, 1):  # around the reference heuristic 32*avg_w/avg_deg (hybrid_sssp.cu:196-197)
-        d = max(1, base_delta // div)
-        modes[f"delta{d}"] = dict(priority="low_high", priority_delta=d, max_iteration=1000000)
-    e_reached, mode_ms, ref0 = {}, {}, None
-    for name, kw in modes.items():
-        ts = []
-        for s in srcs[:2]:
-            out, st, _ = G.sssp(s, **kw)
-            ts.append(st.time_kernel_ms)
-            e_reached[s] = st.edges_reached
-            if ref0 is None:
-                ref0 = out.copy()
-            elif s == srcs[0]:
-                assert (out == ref0).all(), f"mode {name} disagrees"
-        mode_ms[name] = float(np.mean(ts))
-    best = min(mode_ms, key=mode_ms.get)
-    kw = dict(modes[best])
+    # ---- options from the library's autotuner (sg_autotune: mode/delta, blocks
+    # per SM, load balancing, lookahead depth, heavy threshold; every candidate
+    # must reproduce the first one's distances), untimed
+    tuned, tuned_ms, report = G.autotune("sssp", srcs[:2], max_iteration=1000000)
+    kw = dict(tuned, max_iteration=1000000)
+    best = "{variant}{d}".format(variant=tuned["variant"], d=f"_delta{tuned['priority_delta']:g}"
+                                 if "priority" in tuned else "")
+    mode_ms = [dict(r) for r in report]
+    e_reached = {}
     for s in srcs:
         _, st, _ = G.sssp(s, **kw)
         e_reached[s] = st.edges_reached
@@ -343,7 +331,7 @@ def run_ours(a):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         G2 = ctx.graph_from_csr(off_p.data_ptr(), idx_p.data_ptr(), w_p.data_ptr(), nv=nv, ne=ne,
-                                no_csc=best.startswith("delta") or best == "push_dd")
+                                no_csc=tuned["variant"] == "async_push_dd")
         for s in srcs:
             G2.sssp(s, out=host_out.numpy(), **e2e_kw)
         G2.close()
@@ -359,13 +347,14 @@ def run_ours(a):
     peak, peak_kind = peak_hbm()
     avg_launch_ms = float(np.mean(launch_ms))
     achieved = (step_bytes / len(srcs)) / (avg_launch_ms * 1e-3) / 1e9
-    traffic = read_traffic(best)
+    traffic = read_traffic("delta" if "priority" in tuned else "push")
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "nv": nv, "ne": ne, "sources_per_step": len(srcs), "mode": best,
-                   "mode_ms": mode_ms, "edges_reached_per_step": step_edges,
+                   "options": tuned, "autotune_ms_per_source": tuned_ms, "autotune_report": mode_ms,
+                   "edges_reached_per_step": step_edges,
                    "l2": "inputs larger than L2 (graph arrays %.0f MB vs 126 MB L2)" % ((4 * (nv + 1) + 8 * ne) / 1e6),
                    "parallelism": f"replicas{world}"},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -460,29 +449,19 @@ def per_algo(ctx, cache, a):
         cpu_GTEPS=st.edges_reached / cpu_s / 1e9, cpu_ms=1e3 * cpu_s, cpu=cpu_kind)
     G.close()
 
-    # SSSP on the 4096x4096 grid, weights [1,1000): delta picked from three candidates, push DD beside
+    # SSSP on the 4096x4096 grid, weights [1,1000), source 0: options from the autotuner
     h = sg.HostGraph.grid(4096, 4096).gen_weights(1, 1000, 2)
     G = ctx.graph(h, no_csc=True)
     src = 0
-    cand = {"push_dd": dict(variant="async_push_dd")}
-    base = max(1, int(32 * float(h.weights.mean()) / (h.ne / h.nv)))
-    for d in (base // 4, base, base * 4):
-        cand[f"delta{max(1, d)}"] = dict(priority="low_high", priority_delta=max(1, d))
-    times, first, agree = {}, None, True
-    for name, kw in cand.items():
-        d, st, _ = G.sssp(src, max_iteration=10000000, **kw)
-        times[name] = st.time_kernel_ms
-        if first is None:
-            first = d.copy()
-        agree &= bool((d == first).all())
-    best = min(times, key=times.get)
-    t, (d, st, _) = _median_ms(lambda: G.sssp(src, max_iteration=10000000, **cand[best]), 6)
+    tuned, _, report = G.autotune("sssp", [src], max_iteration=10000000)
+    t, (d, st, _) = _median_ms(lambda: G.sssp(src, max_iteration=10000000, **tuned), 6)
     res["sssp_grid4096_w1-1000"] = dict(
-        GTEPS=st.edges_reached / t / 1e6, ms=t, rounds=st.rounds, mode=best, mode_ms=times, modes_agree=agree,
+        GTEPS=st.edges_reached / t / 1e6, ms=t, rounds=st.rounds, options=tuned,
+        autotune_report=report, candidates_agree=all(r["status"] == 0 for r in report),
         us_per_round=1e3 * t / max(1, st.rounds), **_roof(sssp_bytes(h.nv, st.edges_reached), t, peak),
         cpu="not timed: the reference's SSSPHostNaive needs about 4 minutes on one core for this graph")
     G.close()
-    del h, d, first
+    del h, d
 
     # PageRank RMAT-23 directed, FP32, residual 1e-7: data-driven push vs topology-driven pull
     h = sg.HostGraph.rmat(23, 16, seed=1)

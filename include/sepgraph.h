@@ -94,7 +94,10 @@ typedef struct sg_options {
     int32_t blocks_per_sm;    /* resident engine blocks per SM; 0 = library choice by graph size */
     int32_t heavy_degree;     /* push/pull: vertices above this many edges are split into chunks; 0 = 32 */
     int32_t chunk_edges;      /* edges per chunk of a split vertex; 0 = 256 */
-    int32_t reserved[4];
+    int32_t team_blocks;      /* batched launches: blocks per team; 0 = by graph size */
+    int32_t local_depth;      /* push rounds: levels a block follows its own discoveries before the
+                                 round ends (0 = off; functors with ReorderSafe() only) */
+    int32_t reserved[2];
 } sg_options;
 
 /* Per-round trace record (the reference's --trace line, framework.cuh:334-348). */
@@ -189,7 +192,7 @@ typedef struct sg_batch_query {
 } sg_batch_query;
 
 /* Batched SSSP / BFS: n queries over any mix of graphs in ONE cooperative
- * launch.  The grid is split into teams of blocks (sg_options.reserved[0] =
+ * launch.  The grid is split into teams of blocks (sg_options.team_blocks =
  * blocks per team, 0 = by graph size); each team runs one query's whole round
  * loop with its own frontiers and takes the next query (largest graphs first)
  * when done.  Every output equals sg_sssp / sg_bfs for that query.  stats is
@@ -274,15 +277,17 @@ sg_status sg_server_destroy(sg_server *s);
 
 /* ------------------------------------------------------------------ autotuner
  * No counterpart in the reference (its variants, thresholds and grid shape are
- * command-line choices).  Times a fixed set of candidate options for one
- * algorithm (SG_QUERY_*) on the given graph and sources — variant (hybrid
- * policy, forced push, forced pull), SSSP two-level priority delta around the
- * reference heuristic 32*avg_w/avg_deg, blocks per SM and the heavy-vertex
- * split threshold — checks that every candidate gives the same result as the
- * first (bit-exact for BFS/SSSP, L1 <= 1e-6 for PageRank, 1e-4 relative for
- * BC) and writes the fastest to *best (starting from *base, NULL = defaults).
- * report (optional) receives one line per candidate; at most max_candidates
- * entries are timed (0 = all). */
+ * command-line choices).  Times candidate options for one algorithm
+ * (SG_QUERY_*) on the given graph and sources in stages, each keeping the best
+ * so far: the mode (hybrid policy, forced push, forced pull; for SSSP the
+ * two-level priority delta around the reference heuristic 32*avg_w/avg_deg),
+ * then blocks per SM, push load balancing, local lookahead depth (BFS/SSSP)
+ * and the heavy-vertex split threshold.  Every candidate must give the first
+ * candidate's result (bit-exact for BFS/SSSP, PageRank L1 within
+ * max(1e-6, 20 * pr_error), BC 1e-4 relative) before its time counts.  Writes
+ * the fastest to *best (starting from *base, NULL = defaults); report
+ * (optional) receives one line per candidate; at most max_candidates are timed
+ * (0 = 64). */
 typedef struct sg_tune_entry {
     sg_options options;
     double ms;       /* median device time per source */

@@ -12,42 +12,36 @@
 
 namespace {
 
-std::vector<sg_options> candidates(sg_graph *g, int algo, const sg_options &base) {
+// Candidate modes of an algorithm (variant, and for SSSP the two-level priority
+// delta around the reference heuristic 32*avg_w/avg_deg, hybrid_sssp.cu:196-197).
+std::vector<sg_options> modes(sg_graph *g, int algo, const sg_options &base) {
     std::vector<sg_options> out;
-    auto add = [&](int variant, int bps, int heavy, int priority, double delta) {
+    auto add = [&](int variant, int priority, double delta) {
         sg_options o = base;
         o.variant = variant;
-        o.blocks_per_sm = bps;
-        o.heavy_degree = heavy;
         o.priority = priority;
         o.priority_delta = delta;
         o.blocking = 1;
         out.push_back(o);
     };
-    const int bps_set[] = {2, 4, 8};
-    if (algo == SG_QUERY_BFS) {
-        for (int v : {SG_VARIANT_AUTO, SG_ASYNC_PUSH_DD})
-            for (int b : {1, 2, 4, 8})
-                for (int hv : {32, 128}) add(v, b, hv, SG_PRIORITY_NONE, 0);
+    if (algo == SG_QUERY_BFS || algo == SG_QUERY_BC) {
+        add(SG_VARIANT_AUTO, SG_PRIORITY_NONE, 0);
+        add(SG_ASYNC_PUSH_DD, SG_PRIORITY_NONE, 0);
     } else if (algo == SG_QUERY_SSSP) {
         uint32_t nv = 0;
         uint64_t ne = 0;
         sg_graph_info(g, &nv, &ne, nullptr, nullptr);
         const double avg_w = ne ? sgb::graph_weight_sum(g) / (double)ne : 1.0;
         const double avg_deg = nv ? (double)ne / nv : 1.0;
-        const double heuristic = std::max(1.0, std::floor(32.0 * avg_w / std::max(avg_deg, 1e-9)));  // hybrid_sssp.cu:196-197
-        for (int b : bps_set) {
-            add(SG_VARIANT_AUTO, b, 0, SG_PRIORITY_NONE, 0);
-            add(SG_ASYNC_PUSH_DD, b, 0, SG_PRIORITY_NONE, 0);
-            for (double f : {1.0 / 16, 1.0 / 4, 1.0, 4.0})
-                add(SG_ASYNC_PUSH_DD, b, 0, SG_PRIORITY_LOW_HIGH, std::max(1.0, std::floor(heuristic * f)));
-        }
-    } else if (algo == SG_QUERY_PAGERANK) {
-        for (int v : {SG_VARIANT_AUTO, SG_SYNC_PULL_TD, SG_ASYNC_PUSH_DD})
-            for (int b : bps_set) add(v, b, 0, SG_PRIORITY_NONE, 0);
+        const double heuristic = std::max(1.0, std::floor(32.0 * avg_w / std::max(avg_deg, 1e-9)));
+        add(SG_VARIANT_AUTO, SG_PRIORITY_NONE, 0);
+        add(SG_ASYNC_PUSH_DD, SG_PRIORITY_NONE, 0);
+        for (double f : {1.0 / 16, 1.0 / 4, 1.0, 4.0})
+            add(SG_ASYNC_PUSH_DD, SG_PRIORITY_LOW_HIGH, std::max(1.0, std::floor(heuristic * f)));
     } else {
-        for (int v : {SG_VARIANT_AUTO, SG_ASYNC_PUSH_DD})
-            for (int b : bps_set) add(v, b, 0, SG_PRIORITY_NONE, 0);
+        add(SG_VARIANT_AUTO, SG_PRIORITY_NONE, 0);
+        add(SG_SYNC_PULL_TD, SG_PRIORITY_NONE, 0);
+        add(SG_ASYNC_PUSH_DD, SG_PRIORITY_NONE, 0);
     }
     return out;
 }
@@ -101,12 +95,17 @@ bool same(int algo, const Result &a, const Result &b, double pr_error) {
 
 }  // namespace
 
+// Staged search: the mode first, then, keeping the best so far, blocks per
+// SM, push load balancing, local lookahead depth (BFS/SSSP) and the
+// heavy-vertex split threshold.  Every candidate must reproduce the first
+// candidate's result before its time counts.
 extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources, uint32_t nsrc, const sg_options *base,
                                  uint32_t max_candidates, sg_options *best, double *best_ms, sg_tune_entry *report,
                                  uint32_t report_capacity, uint32_t *n_report) {
     if (!g || !best || algo < SG_QUERY_BFS || algo > SG_QUERY_BC) return SG_ERR_INVALID_ARG;
     uint32_t nv = 0;
-    sg_status st = sg_graph_info(g, &nv, nullptr, nullptr, nullptr);
+    uint64_t ne = 0;
+    sg_status st = sg_graph_info(g, &nv, &ne, nullptr, nullptr);
     if (st != SG_OK) return st;
     const bool sourceless = algo == SG_QUERY_PAGERANK;
     if (!sourceless && (!sources || nsrc == 0)) return SG_ERR_INVALID_ARG;
@@ -117,20 +116,24 @@ extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources,
         b0 = *base;
     else
         sg_options_default(&b0);
-    std::vector<sg_options> cand = candidates(g, algo, b0);
-    if (max_candidates && cand.size() > max_candidates) cand.resize(max_candidates);
     const uint32_t runs = sourceless ? 1u : nsrc;
+    const uint32_t limit = max_candidates ? max_candidates : 64u;
     std::vector<Result> ref(runs);
     bool have_ref = false;
     double best_t = -1;
+    uint32_t tried = 0;
     if (n_report) *n_report = 0;
-    for (size_t c = 0; c < cand.size(); ++c) {
+
+    // times one candidate; returns its median ms or -1 when it failed or differed
+    auto trial = [&](const sg_options &cand) -> double {
+        if (tried >= limit) return -1;
+        ++tried;
         std::vector<double> ts;
         sg_status cs = SG_OK;
         std::vector<Result> res(runs);
         for (uint32_t k = 0; k < runs && cs == SG_OK; ++k) {
             double ms = 0;
-            cs = run_one(g, algo, sourceless ? 0u : sources[k], cand[c], nv, res[k], &ms);
+            cs = run_one(g, algo, sourceless ? 0u : sources[k], cand, nv, res[k], &ms);
             ts.push_back(ms);
         }
         if (cs == SG_OK) {
@@ -147,19 +150,53 @@ extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources,
             std::sort(ts.begin(), ts.end());
             med = ts[ts.size() / 2];
         }
-        if (cs == SG_OK && (best_t < 0 || med < best_t)) {
-            best_t = med;
-            *best = cand[c];
-        }
         if (report && n_report && *n_report < report_capacity) {
             sg_tune_entry &e = report[(*n_report)++];
-            e.options = cand[c];
+            e.options = cand;
             e.ms = med;
             e.status = cs;
             e.pad = 0;
         }
-    }
+        if (cs != SG_OK) return -1;
+        if (best_t < 0 || med < best_t) {
+            best_t = med;
+            *best = cand;
+        }
+        return med;
+    };
+
+    for (const sg_options &m : modes(g, algo, b0)) trial(m);
     if (best_t < 0) return SG_ERR_UNSUPPORTED;  // no candidate finished
+    const bool push_mode = best->variant == SG_VARIANT_AUTO || best->variant == SG_ASYNC_PUSH_DD;
+    {
+        const sg_options cur = *best;
+        for (int b : {1, 2, 4, 8}) {
+            sg_options c = cur;
+            c.blocks_per_sm = b;
+            trial(c);
+        }
+    }
+    if (push_mode && algo != SG_QUERY_PAGERANK) {
+        const sg_options cur = *best;
+        const double avg_deg = nv ? (double)ne / nv : 0;
+        sg_options c = cur;  // the other of the two load-balancing modes the automatic rule picks from
+        c.lb_push = avg_deg >= 5 ? SG_LB_NONE : SG_LB_FINE_GRAINED;
+        trial(c);
+    }
+    if (push_mode && (algo == SG_QUERY_BFS || algo == SG_QUERY_SSSP)) {
+        const sg_options cur = *best;
+        for (int d : {4, 16}) {
+            sg_options c = cur;
+            c.local_depth = d;
+            trial(c);
+        }
+    }
+    if (push_mode && algo != SG_QUERY_PAGERANK) {
+        const sg_options cur = *best;
+        sg_options c = cur;
+        c.heavy_degree = 128;
+        trial(c);
+    }
     if (best_ms) *best_ms = best_t;
     return SG_OK;
 }

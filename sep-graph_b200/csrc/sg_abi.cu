@@ -113,6 +113,7 @@ sgb::EngineConfig make_config(const sg_graph *g, const sg_options &o, int scheme
     c.blocks_per_sm = o.blocks_per_sm;
     if (o.heavy_degree > 0) c.heavy_degree = (uint32_t)o.heavy_degree;
     if (o.chunk_edges > 0) c.chunk_edges = (uint32_t)o.chunk_edges;
+    if (o.local_depth > 0) c.local_depth = (uint32_t)o.local_depth;
     c.blocking = o.blocking != 0;
     if (o.trace && stats && stats->trace && stats->trace_capacity) {
         c.trace = 1;
@@ -436,7 +437,8 @@ sg_status sg_bfs(sg_graph *g, uint32_t source, const sg_options *opt, uint32_t *
     else
         SG_TRY_CUDA(ctx, g->ws.get("value_u32", g->nv, &value));
     SG_TRY_CUDA(ctx, g->ws.get("buffer_u32", g->nv, &buffer));
-    apps::BFS<uint32_t, uint32_t, graphs::NoWeight> app(source, o.non_atomic != 0);
+    // local lookahead mixes levels inside a round, which needs the atomic minimum
+    apps::BFS<uint32_t, uint32_t, graphs::NoWeight> app(source, o.non_atomic != 0 && o.local_depth <= 0);
     sgb::EngineResult res;
     sg_status st = sgb::run_engine<decltype(app), uint32_t, uint32_t, graphs::NoWeight>(g, app, cfg, value, buffer, &res);
     if (st == SG_OK) st = deliver(ctx, levels_out, value, g->nv, out_dev);

@@ -573,8 +573,8 @@ sg_status prepare_batch(sg_ctx *ctx, sgb::Workspace &ws, std::vector<engine::Bat
     // BFS/SSSP queries on RMAT scale 22 ran fastest with 37-74 blocks per team,
     // 1.8x faster than one grid-wide team), and never fewer blocks than it
     // takes to keep the whole grid busy when the batch has few queries.
-    uint32_t team_blocks = (uint32_t)o.reserved[0];
-    if (o.reserved[0] <= 0) {
+    uint32_t team_blocks = (uint32_t)o.team_blocks;
+    if (o.team_blocks <= 0) {
         team_blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ne_max >> 21, total_blocks));
         team_blocks = std::max(team_blocks, total_blocks / n);
     }
@@ -820,6 +820,7 @@ engine::Params batch_params(const sg_options &o, int scheme) {
     p.heavy_threshold = o.heavy_degree > 0 ? (uint32_t)o.heavy_degree : 32u;
     p.chunk_edges = o.chunk_edges > 0 ? (uint32_t)std::max(32, o.chunk_edges) : 256u;
     p.pull_warp_threshold = 32;
+    p.local_depth = o.local_depth > 0 ? (uint32_t)o.local_depth : 0u;
     p.alpha = o.alpha;
     p.beta = o.beta > 0 ? o.beta : 18;
     p.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
@@ -920,7 +921,7 @@ sg_status dispatch_batch(int algo, const sg_batch_query *q, uint32_t n, const sg
     }
     if (algo == SG_QUERY_BFS) {
         using App = apps::BFS<uint32_t, uint32_t, graphs::NoWeight>;
-        const bool non_atomic = o.non_atomic != 0;
+        const bool non_atomic = o.non_atomic != 0 && o.local_depth <= 0;  // lookahead needs the atomic minimum
         auto qs = build([non_atomic](uint32_t s) { return App(s, non_atomic); }, (App *)nullptr);
         return run.template go<App, uint32_t, uint32_t, graphs::NoWeight>(qs, graphs, outs, p);
     }

@@ -116,6 +116,7 @@ struct Params {
     uint32_t heavy_threshold;
     uint32_t chunk_edges;
     uint32_t pull_warp_threshold;
+    uint32_t local_depth;  // levels a block follows its own discoveries inside a push round (0 = off)
     double alpha, beta;
     long long total_workload0;
     unsigned long long prio_init_raw, prio_step_raw;
@@ -168,6 +169,18 @@ struct WarpLB {
     uint32_t beg[32];
     uint32_t src[32];
     TBuffer pay[32];
+};
+
+// A block's own queue of vertices it discovered in a push round and may
+// process before the round ends (local lookahead, reorder-safe functors only).
+// Two buffers alternate between "being processed" and "being filled"; what
+// does not fit, and what is left when the depth runs out, goes to the global
+// worklist.
+constexpr uint32_t kLocalCap = 1024;
+struct LocalQ {
+    uint32_t item[2][kLocalCap];
+    uint32_t n[2];
+    uint32_t out;  // buffer receiving discoveries
 };
 
 // Per-thread accumulators flushed once per phase.
@@ -374,12 +387,31 @@ struct EngineKernel {
     // bits of an output slot only, so a vertex improved during a round always
     // reaches the next round's worklist (which reads it after the barrier) and
     // no fence is needed between the state update and the queued bit.
+    // With a block queue `lq`, near (high-priority) vertices go there first.
     // All 32 lanes must call.
     static __device__ __forceinline__ void enqueue(App &app, const Args &a, const Snap &s, uint32_t dst, bool want,
-                                                   Acc &acc) {
+                                                   Acc &acc, LocalQ *lq = nullptr) {
         Counters *n = &a.ctrl->cnt;
         bool hi = true;
         if (a.p.priority && want) hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), dev::ld_l2(a.buffer + dst));
+        if (lq) {
+            bool loc = want && hi;
+            const uint32_t m = __ballot_sync(dev::kFullMask, loc);
+            if (m) {
+                const uint32_t lane = dev::lane_id(), leader = __ffs(m) - 1, o = lq->out;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(&lq->n[o], (uint32_t)__popc(m));
+                base = __shfl_sync(dev::kFullMask, base, leader);
+                if (loc) {
+                    const uint32_t pos = base + __popc(m & dev::lanemask_lt());
+                    if (pos < kLocalCap)
+                        lq->item[o][pos] = dst;
+                    else
+                        loc = false;  // block queue full: global worklist
+                }
+            }
+            want = want && !loc;
+        }
         bool w_hi = want && hi, w_lo = want && !hi;
         if (w_hi) w_hi = dev::bitmap_set(a.qflag[s.qhi], dst);
         if (w_lo) w_lo = dev::bitmap_set(a.qflag[s.qlo], dst);
@@ -390,10 +422,18 @@ struct EngineKernel {
 
     // Single-thread enqueue (LB NONE paths run divergent per-thread loops).
     static __device__ __forceinline__ void enqueue_one(App &app, const Args &a, const Snap &s, uint32_t dst,
-                                                       Acc &acc) {
+                                                       Acc &acc, LocalQ *lq = nullptr) {
         Counters *n = &a.ctrl->cnt;
         bool hi = true;
         if (a.p.priority) hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), dev::ld_l2(a.buffer + dst));
+        if (lq && hi) {
+            const uint32_t o = lq->out;
+            const uint32_t pos = atomicAdd(&lq->n[o], 1u);
+            if (pos < kLocalCap) {
+                lq->item[o][pos] = dst;
+                return;
+            }
+        }
         const uint32_t q = hi ? s.qhi : s.qlo;
         if (!dev::bitmap_set(a.qflag[q], dst)) return;
         const uint32_t pos = atomicAdd(&n->qcount[q], 1u);
@@ -456,7 +496,8 @@ struct EngineKernel {
     // the warp walks the concatenation of their edge lists 32 edges at a time.
     // All 32 lanes must call.
     static __device__ void expand_warp(App &app, const Args &a, const Snap &s, WarpLB<TB> &w, uint32_t src,
-                                       uint32_t beg, uint32_t deg, TB payload, bool dd, Acc &acc) {
+                                       uint32_t beg, uint32_t deg, TB payload, bool dd, Acc &acc,
+                                       LocalQ *lq = nullptr) {
         const uint32_t lane = dev::lane_id();
         const uint32_t incl = dev::warp_inclusive_scan(deg);
         const uint32_t total = __shfl_sync(dev::kFullMask, incl, 31);
@@ -477,7 +518,7 @@ struct EngineKernel {
                 const int st = accumulate_w(app, cur.src, cur.dst, cur.wt, a.buffer + cur.dst, cur.pay);
                 want = dd && acc_success(st);
             }
-            enqueue(app, a, s, cur.dst, want, acc);
+            enqueue(app, a, s, cur.dst, want, acc, lq);
             cur = nxt;
         }
         if (lane == 0) acc.edges += total;
@@ -525,12 +566,12 @@ struct EngineKernel {
     // Thread-per-vertex sequential expansion honouring BREAK (LB NONE,
     // async_push_dd.cuh:24-77).
     static __device__ void expand_serial(App &app, const Args &a, const Snap &s, uint32_t src, uint32_t beg,
-                                         uint32_t deg, TB payload, bool dd, Acc &acc) {
+                                         uint32_t deg, TB payload, bool dd, Acc &acc, LocalQ *lq = nullptr) {
         uint32_t e = beg;
         for (; e < beg + deg; ++e) {
             const uint32_t dst = a.csr.edge_dest(e);
             const int st = accumulate<App, TB, TW>(app, a.csr_w, src, dst, e, a.buffer + dst, payload);
-            if (dd && acc_success(st)) enqueue_one(app, a, s, dst, acc);
+            if (dd && acc_success(st)) enqueue_one(app, a, s, dst, acc, lq);
             if (!acc_continue(st)) {
                 ++e;
                 break;
@@ -605,7 +646,7 @@ struct EngineKernel {
     // ---------------------------------------------------------------- push
     // Phase A of a push round over worklist items (DD) or all vertices (TD).
     static __device__ void push_phase_a(App &app, const Args &a, const Snap &s, WarpLB<TB> &wlb, bool dd,
-                                        int lb, Acc &acc) {
+                                        int lb, Acc &acc, LocalQ *lq = nullptr) {
         const uint32_t lane = dev::lane_id();
         const uint32_t N = dd ? s.F : a.csr.nnodes;
         const uint32_t *Q = a.queue[s.qin];
@@ -648,13 +689,70 @@ struct EngineKernel {
             }
             uint32_t deg = sched ? end - beg : 0u;
             if (lb == LB_NONE) {
-                if (deg) expand_serial(app, a, s, v, beg, deg, payload, dd, acc);
+                if (deg) expand_serial(app, a, s, v, beg, deg, payload, dd, acc, lq);
                 continue;
             }
             const bool heavy = deg > a.p.heavy_threshold;
             register_heavy(a, s.round & 1u, heavy, v, beg, deg, payload);
             if (heavy) deg = 0;
-            expand_warp(app, a, s, wlb, v, beg, deg, payload, dd, acc);
+            expand_warp(app, a, s, wlb, v, beg, deg, payload, dd, acc, lq);
+        }
+        if (lq) local_levels(app, a, s, wlb, lb, acc, lq);
+    }
+
+    // Local lookahead: the block processes the vertices it discovered itself,
+    // up to local_depth levels deep, without waiting for the round's barrier
+    // (reorder-safe functors: any order of pushes reaches the same result).
+    // Heavy vertices are left to the worklist uncombined, so that a later round
+    // splits them into chunks; whatever is still queued at the end goes to the
+    // worklist too.  Every thread of the block must call.
+    static __device__ void local_levels(App &app, const Args &a, const Snap &s, WarpLB<TB> &wlb, int lb, Acc &acc,
+                                        LocalQ *lq) {
+        const uint32_t lane = dev::lane_id(), warp = dev::warp_id();
+        for (uint32_t d = 0; d < a.p.local_depth; ++d) {
+            __syncthreads();
+            const uint32_t in = lq->out;
+            const uint32_t cnt = min(lq->n[in], kLocalCap);
+            __syncthreads();
+            if (cnt == 0) return;  // the same values in every thread
+            if (threadIdx.x == 0) {
+                lq->out = in ^ 1u;
+                lq->n[in ^ 1u] = 0;
+            }
+            __syncthreads();
+            for (uint32_t base = warp * 32; base < cnt; base += kWarpsPerBlock * 32) {
+                const uint32_t i = base + lane;
+                const bool valid = i < cnt;
+                const uint32_t v = valid ? lq->item[in][i] : 0u;
+                uint32_t beg = 0, end = 0;
+                if (valid) {
+                    beg = a.csr.begin_edge(v);
+                    end = a.csr.end_edge(v);
+                }
+                const bool heavy = valid && lb != LB_NONE && end - beg > a.p.heavy_threshold;
+                enqueue(app, a, s, v, heavy, acc);
+                TB payload{};
+                bool sched = false;
+                if (valid && !heavy) {
+                    auto pr = app.App::CombineValueBuffer(v, a.value + v, a.buffer + v);
+                    payload = pr.first;
+                    sched = pr.second;
+                }
+                const uint32_t deg = sched ? end - beg : 0u;
+                if (lb == LB_NONE) {
+                    if (deg) expand_serial(app, a, s, v, beg, deg, payload, true, acc, lq);
+                    continue;
+                }
+                expand_warp(app, a, s, wlb, v, beg, deg, payload, true, acc, lq);
+            }
+        }
+        __syncthreads();
+        const uint32_t in = lq->out;
+        const uint32_t cnt = min(lq->n[in], kLocalCap);
+        for (uint32_t base = warp * 32; base < cnt; base += kWarpsPerBlock * 32) {
+            const uint32_t i = base + lane;
+            const bool valid = i < cnt;
+            enqueue(app, a, s, valid ? lq->item[in][i] : 0u, valid, acc);
         }
     }
 
@@ -1101,6 +1199,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
     using K = EngineKernel<App, TV, TB, TW>;
     __shared__ RoundState s;
     __shared__ WarpLB<TB> wlb[kWarpsPerBlock];
+    __shared__ LocalQ lq_block;
     App app = app_in;
     Ctrl *c = a.ctrl;
     const unsigned long long tmo = a.p.timeout_ns;
@@ -1147,7 +1246,16 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         switch (var) {
             case V_ASYNC_PUSH_DD: {
                 K::clear_dirty(a, s);
-                K::push_phase_a(app, a, s, my_lb, true, lb_push, acc);
+                LocalQ *lq = nullptr;
+                if (a.p.local_depth > 0 && reorder_safe(app)) {
+                    if (threadIdx.x == 0) {
+                        lq_block.out = 0;
+                        lq_block.n[0] = lq_block.n[1] = 0;
+                    }
+                    __syncthreads();
+                    lq = &lq_block;
+                }
+                K::push_phase_a(app, a, s, my_lb, true, lb_push, acc, lq);
                 if (!K::defer_chunks(app, a) && s.heavy_expected > 0 && lb_push != LB_NONE) {
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                     if (!grid_sync(c, tmo, nop)) return false;

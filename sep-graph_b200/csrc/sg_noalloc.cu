@@ -177,12 +177,13 @@ extern "C" sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *ind
     p.heavy_threshold = kHeavyDegree;
     p.chunk_edges = kChunkEdges;
     p.pull_warp_threshold = 32;
+    p.local_depth = o.local_depth > 0 ? (uint32_t)o.local_depth : 0u;
     p.alpha = o.alpha;
     p.beta = o.beta > 0 ? o.beta : 18;
     p.total_workload0 = (long long)((double)ne * (o.edge_factor > 0 ? o.edge_factor : 1.0));
     p.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
 
-    BfsApp app(source, o.non_atomic != 0);
+    BfsApp app(source, o.non_atomic != 0 && o.local_depth <= 0);  // lookahead needs the atomic minimum
     app.m_csr_graph = a.csr;
     app.m_csc_graph = a.csc;
     app.m_nnodes = nv;

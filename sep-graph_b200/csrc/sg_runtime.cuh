@@ -157,6 +157,7 @@ struct EngineConfig {
     int blocks_per_sm = 0;
     uint32_t heavy_degree = 32;  // out/in-degree above which a vertex is split into chunks
     uint32_t chunk_edges = 256;
+    uint32_t local_depth = 0;  // local lookahead levels in push rounds (0 = off)
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -261,6 +262,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     p.heavy_threshold = heavy_threshold;
     p.chunk_edges = chunk_edges;
     p.pull_warp_threshold = 32;
+    p.local_depth = cfg.local_depth;
     p.alpha = cfg.alpha;
     p.beta = cfg.beta;
     p.total_workload0 = (long long)((double)ne * cfg.edge_factor);

@@ -52,7 +52,8 @@ class Options(C.Structure):
         ("beta", C.c_double), ("edge_factor", C.c_double), ("max_iteration", C.c_int32), ("fused", C.c_int32),
         ("block_size", C.c_int32), ("non_atomic", C.c_int32), ("trace", C.c_int32), ("pr_error", C.c_double),
         ("timeout_s", C.c_double), ("blocking", C.c_int32), ("blocks_per_sm", C.c_int32),
-        ("heavy_degree", C.c_int32), ("chunk_edges", C.c_int32), ("reserved", C.c_int32 * 4),
+        ("heavy_degree", C.c_int32), ("chunk_edges", C.c_int32), ("team_blocks", C.c_int32),
+        ("local_depth", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -60,7 +61,7 @@ class TuneEntry(C.Structure):
     _fields_ = [("options", Options), ("ms", C.c_double), ("status", C.c_int32), ("pad", C.c_int32)]
 
 
-TUNED_FIELDS = ("variant", "blocks_per_sm", "heavy_degree", "priority", "priority_delta")
+TUNED_FIELDS = ("variant", "blocks_per_sm", "heavy_degree", "priority", "priority_delta", "lb_push", "local_depth")
 VARIANT_NAMES = {-1: "auto", 0: "sync_push_td", 1: "sync_push_dd", 2: "sync_pull_td", 3: "sync_pull_dd",
                  4: "async_push_td", 5: "async_push_dd", 6: "async_pull_td", 7: "async_pull_dd"}
 
@@ -407,7 +408,7 @@ class Context:
             arr[i].out = _ptr(o)
         o = make_options(**opts)
         if team_blocks:
-            o.reserved[0] = int(team_blocks)
+            o.team_blocks = int(team_blocks)
         st = Stats()
         per = (C.c_float * n)()
         _check(fn(self._c, arr, n, C.byref(o), C.byref(st), per), name, self._c)
@@ -477,7 +478,7 @@ class BatchPlan:
             arr[i].out = _ptr(o)
         o = make_options(**opts)
         if team_blocks:
-            o.reserved[0] = int(team_blocks)
+            o.team_blocks = int(team_blocks)
         self.ctx, self.n, self._outs = ctx, n, list(outs)
         self._p = _P()
         _check(load().sg_batch_plan_create(ctx.handle, QUERY_ALGOS[algo], arr, n, C.byref(o), C.byref(self._p)),
