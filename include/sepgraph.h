@@ -95,8 +95,9 @@ typedef struct sg_options {
     int32_t heavy_degree;     /* push/pull: vertices above this many edges are split into chunks; 0 = 32 */
     int32_t chunk_edges;      /* edges per chunk of a split vertex; 0 = 256 */
     int32_t team_blocks;      /* batched launches: blocks per team; 0 = by graph size */
-    int32_t local_depth;      /* push rounds: levels a block follows its own discoveries before the
-                                 round ends (0 = off; functors with ReorderSafe() only) */
+    int32_t local_depth;      /* levels a block follows its own discoveries before a round ends
+                                 (0 = off; with variant SG_ASYNC_PUSH_DD and functors whose
+                                 ReorderSafe() holds only) */
     int32_t reserved[2];
 } sg_options;
 
@@ -245,7 +246,7 @@ typedef struct sg_server_config {
     uint32_t max_batch;        /* queries per batch (default 256) */
     uint32_t max_pending;      /* submit returns SG_ERR_BUSY beyond this (default 1<<20) */
     uint32_t msbfs_min;        /* BFS queries of one graph that go to multi-source BFS (default 4) */
-    uint32_t sssp_delta;       /* 0: SSSP as ASYNC_PUSH_DD; >0: two-level priority with this delta */
+    uint32_t sssp_delta;       /* SSSP two-level priority delta; 0 = each graph's 32*avg_w/avg_deg */
     uint32_t pad;
     double pr_error;           /* PageRank residual threshold (default 1e-7) */
     int32_t reserved[8];

@@ -88,18 +88,34 @@ sg_options server_options(const sg_server_config &c, int algo) {
     o.max_iteration = 1000000;
     o.blocks_per_sm = std::max(1u, 6u / std::max(1u, c.slots));  // slots share the SMs
     if (algo == SG_QUERY_SSSP) {
-        if (c.sssp_delta) {
-            o.priority = SG_PRIORITY_LOW_HIGH;
-            o.priority_delta = c.sssp_delta;
-        } else {
-            o.variant = SG_ASYNC_PUSH_DD;
-        }
+        // two-level priority (delta-stepping) with the configured delta, or with
+        // each graph's own reference heuristic 32*avg_w/avg_deg when it is 0
+        o.priority = SG_PRIORITY_LOW_HIGH;
+        o.priority_delta = c.sssp_delta;
     }
     if (algo == SG_QUERY_PAGERANK) {
         o.pr_error = c.pr_error;
         o.max_iteration = 100000;
     }
     return o;
+}
+
+}  // namespace
+
+namespace {
+
+// Runs q as one batched launch; a batch that fails as a whole (one query's
+// path counts overflow uint64, say) runs again one query at a time, so that
+// only the failing queries report the error.  idx[k] is q[k]'s slot in status.
+template <typename Call>
+void run_isolated(const std::vector<sg_batch_query> &q, const std::vector<size_t> &idx, std::vector<sg_status> &status,
+                  Call &&call) {
+    const sg_status st = call(q.data(), (uint32_t)q.size());
+    if (st == SG_OK || q.size() == 1) {
+        for (size_t i : idx) status[i] = st;
+        return;
+    }
+    for (size_t k = 0; k < q.size(); ++k) status[idx[k]] = call(&q[k], 1u);
 }
 
 }  // namespace
@@ -160,14 +176,20 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
             std::vector<sg_batch_query> q(rest.size());
             for (size_t k = 0; k < rest.size(); ++k)
                 q[k] = {graphs[b[rest[k]].q.graph_id].g, b[rest[k]].q.source, 0, b[rest[k]].q.out};
-            const sg_status st = sg_bfs_batch(ctx, q.data(), (uint32_t)q.size(), &o, nullptr, nullptr);
-            for (size_t k : rest) status[k] = st;
+            run_isolated(q, rest, status, [&](const sg_batch_query *qq, uint32_t n) {
+                return sg_bfs_batch(ctx, qq, n, &o, nullptr, nullptr);
+            });
         }
     } else if (algo == SG_QUERY_SSSP) {
         std::vector<sg_batch_query> q(b.size());
-        for (size_t k = 0; k < b.size(); ++k) q[k] = {graphs[b[k].q.graph_id].g, b[k].q.source, 0, b[k].q.out};
-        const sg_status st = sg_sssp_batch(ctx, q.data(), (uint32_t)q.size(), &o, nullptr, nullptr);
-        std::fill(status.begin(), status.end(), st);
+        std::vector<size_t> all(b.size());
+        for (size_t k = 0; k < b.size(); ++k) {
+            q[k] = {graphs[b[k].q.graph_id].g, b[k].q.source, 0, b[k].q.out};
+            all[k] = k;
+        }
+        run_isolated(q, all, status, [&](const sg_batch_query *qq, uint32_t n) {
+            return sg_sssp_batch(ctx, qq, n, &o, nullptr, nullptr);
+        });
     } else if (algo == SG_QUERY_PAGERANK) {
         // PageRank has no source: one run per graph answers all its queries
         std::map<uint32_t, std::vector<size_t>> by_graph;
@@ -200,10 +222,10 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
                 in_batch.push_back(i);
             }
         }
-        if (!q.empty()) {
-            const sg_status st = sg_bc_batch(ctx, q.data(), (uint32_t)q.size(), &o, nullptr, nullptr);
-            for (size_t i : in_batch) status[i] = st;
-        }
+        if (!q.empty())
+            run_isolated(q, in_batch, status, [&](const sg_batch_query *qq, uint32_t n) {
+                return sg_bc_batch(ctx, qq, n, &o, nullptr, nullptr);
+            });
     }
 }
 

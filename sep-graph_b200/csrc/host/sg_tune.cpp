@@ -188,6 +188,7 @@ extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources,
         for (int d : {4, 16}) {
             sg_options c = cur;
             c.local_depth = d;
+            c.variant = SG_ASYNC_PUSH_DD;  // the engine follows discoveries under forced push only
             trial(c);
         }
     }

@@ -7,7 +7,10 @@
 // every missing bit is covered), then fix the newly seen bits, write their
 // levels and build the next active list.  A vertex reached by several
 // sources in the same round is expanded once for all of them, so 64 BFSs cost
-// a few passes over the graph instead of 64.  The direction switch uses the
+// a few passes over the graph instead of 64.  Work is balanced in three tiers
+// by degree: a thread per vertex up to 32 edges, a warp per vertex up to 2048,
+// and 2048-edge chunks of bigger vertices (listed once per launch) spread over
+// all warps, so one hub never holds up a round.  The direction switch uses the
 // single-source engine's rule (scout count against unexplored edges / alpha,
 // include/framework/hybrid_policy.h:265-288).  No reference counterpart: the
 // reference runs one source per Engine.
@@ -32,7 +35,8 @@ using namespace sepgraph;
 using engine::Ctrl;
 
 constexpr int kMsThreads = 256;
-constexpr uint32_t kMsBig = 256;  // vertices above this degree are expanded by a whole warp
+constexpr uint32_t kMsWarp = 32;     // vertices above this degree are scanned by a whole warp
+constexpr uint32_t kMsChunk = 2048;  // vertices above this degree are split into chunks of this many edges
 
 struct MsArgs {
     const uint32_t *row, *col;    // CSR
@@ -43,6 +47,13 @@ struct MsArgs {
     uint32_t *active[2], *touched;
     const uint32_t *sources;
     uint32_t *levels;  // nsrc rows of nv
+    // Chunks (v, first edge, edges, -) of the vertices above kMsChunk out-edges
+    // (CSR, [0]) and in-edges (CSC, [1]), listed once at the start of the
+    // launch; every round spreads them over all warps (push: chunks of frontier
+    // vertices, pull: chunks of vertices that still miss a source).
+    uint4 *chunks[2];
+    uint32_t chunk_cap;
+    uint32_t *n_chunks;  // [2], zero at launch
     Ctrl *ctrl;
     uint32_t max_rounds;
     double alpha;
@@ -81,6 +92,21 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
     }
     const uint64_t total_lv = (uint64_t)a.nsrc * a.nv;
     for (uint64_t k = gthread(); k < total_lv; k += nthreads()) a.levels[k] = 0xffffffffu;
+    for (uint32_t v = gthread(); v < a.nv; v += nthreads()) {
+        for (int dir = 0; dir < 2; ++dir) {
+            const uint32_t *off = dir == 0 ? a.row : a.crow;
+            const uint32_t b = __ldg(off + v), deg = __ldg(off + v + 1) - b;
+            if (deg <= kMsChunk) continue;
+            const uint32_t nch = (deg + kMsChunk - 1) / kMsChunk;
+            const uint32_t c0 = atomicAdd(a.n_chunks + dir, nch);
+            for (uint32_t k = 0; k < nch; ++k) {
+                if (c0 + k < a.chunk_cap)
+                    a.chunks[dir][c0 + k] = make_uint4(v, b + k * kMsChunk, min(kMsChunk, deg - k * kMsChunk), 0);
+                else
+                    atomicOr(&n->error, dev::kErrChunkCapacity);
+            }
+        }
+    }
     if (!engine::grid_sync(c, a.timeout_ns, nop)) return;
     if (gthread() < a.nsrc) {
         const uint32_t v = a.sources[gthread()];
@@ -112,6 +138,20 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
         const unsigned long long *F = a.fr[cur];
         unsigned long long edges = 0;
         // ---- phase 1: expand
+        // OR a frontier mask into a neighbour; its first writer lists it for phase 2
+        auto push_to = [&](uint32_t u, unsigned long long f) {
+            const unsigned long long add = f & ~__ldcg(a.seen + u);
+            if (add && (__ldcg(a.next + u) & add) != add) {
+                const unsigned long long old = atomicOr(a.next + u, add);
+                if (old == 0) a.touched[atomicAdd(&n->middle_count, 1u)] = u;
+            }
+        };
+        auto warp_or = [](unsigned long long x) {
+            for (int d = 16; d > 0; d >>= 1) x |= __shfl_xor_sync(dev::kFullMask, x, d);
+            return x;
+        };
+        const uint32_t n_ch = min(__ldcg(a.n_chunks + s.variant), a.chunk_cap);
+        const uint4 *chunks = a.chunks[s.variant];
         if (s.variant == 0) {
             const uint32_t *act = a.active[cur];
             for (uint32_t base = gw * 32; base < s.F; base += nw * 32) {
@@ -124,54 +164,103 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
                     beg = __ldg(a.row + v);
                     deg = __ldg(a.row + v + 1) - beg;
                 }
-                const bool big = deg > kMsBig;
-                if (!big) {
-                    for (uint32_t e = beg; e < beg + deg; ++e) {
-                        const uint32_t u = __ldg(a.col + e);
-                        const unsigned long long add = f & ~__ldcg(a.seen + u);
-                        if (add && (__ldcg(a.next + u) & add) != add) {
-                            const unsigned long long old = atomicOr(a.next + u, add);
-                            if (old == 0) a.touched[atomicAdd(&n->middle_count, 1u)] = u;
-                        }
-                    }
+                if (deg > kMsChunk) deg = 0;  // its chunks are expanded below
+                const bool mid = deg > kMsWarp;
+                if (!mid) {
+                    for (uint32_t e = beg; e < beg + deg; ++e) push_to(__ldg(a.col + e), f);
                     edges += deg;
                 }
-                uint32_t m = __ballot_sync(dev::kFullMask, big);
+                uint32_t m = __ballot_sync(dev::kFullMask, mid);
                 while (m) {
                     const uint32_t j = __ffs(m) - 1;
                     m &= m - 1;
                     const uint32_t bj = __shfl_sync(dev::kFullMask, beg, j), dj = __shfl_sync(dev::kFullMask, deg, j);
                     const unsigned long long fj = __shfl_sync(dev::kFullMask, f, j);
-                    for (uint32_t k = lane; k < dj; k += 32) {
-                        const uint32_t u = __ldg(a.col + bj + k);
-                        const unsigned long long add = fj & ~__ldcg(a.seen + u);
-                        if (add && (__ldcg(a.next + u) & add) != add) {
-                            const unsigned long long old = atomicOr(a.next + u, add);
-                            if (old == 0) a.touched[atomicAdd(&n->middle_count, 1u)] = u;
-                        }
-                    }
+                    for (uint32_t k = lane; k < dj; k += 32) push_to(__ldg(a.col + bj + k), fj);
                     if (lane == 0) edges += dj;
                 }
             }
+            for (uint32_t ch = gw; ch < n_ch; ch += nw) {
+                const uint4 c4 = chunks[ch];
+                const unsigned long long f = __ldcg(F + c4.x);
+                if (!f) continue;  // not in this round's frontier
+                for (uint32_t k = lane; k < c4.z; k += 32) push_to(__ldg(a.col + c4.y + k), f);
+                if (lane == 0) edges += c4.z;
+            }
         } else {
-            // pull: every vertex that misses a source ORs its in-neighbours' frontier masks
-            for (uint32_t u = gthread(); u < a.nv; u += nthreads()) {
-                const unsigned long long miss = a.full & ~__ldcg(a.seen + u);
-                if (!miss) continue;
-                unsigned long long acc = 0;
-                const uint32_t b = __ldg(a.crow + u), e = __ldg(a.crow + u + 1);
-                uint32_t k = b;
-                for (; k < e; ++k) {
-                    acc |= __ldcg(F + __ldg(a.ccol + k));
-                    if ((acc & miss) == miss) {
-                        ++k;
-                        break;
+            // pull: every vertex that misses a source ORs its in-neighbours'
+            // frontier masks, stopping once every missing bit is covered
+            for (uint32_t base = gw * 32; base < a.nv; base += nw * 32) {
+                const uint32_t u = base + lane;
+                unsigned long long miss = 0;
+                uint32_t b = 0, deg = 0;
+                if (u < a.nv) {
+                    miss = a.full & ~__ldcg(a.seen + u);
+                    if (miss) {
+                        b = __ldg(a.crow + u);
+                        deg = __ldg(a.crow + u + 1) - b;
+                        if (deg > kMsChunk) miss = 0;  // its chunks are scanned below
                     }
                 }
-                edges += k - b;
-                if (acc & miss) {
-                    a.next[u] = acc & miss;
-                    a.touched[atomicAdd(&n->middle_count, 1u)] = u;
+                const bool mid = miss && deg > kMsWarp;
+                if (miss && !mid) {
+                    unsigned long long acc = 0;
+                    uint32_t k = b;
+                    for (; k < b + deg; ++k) {
+                        acc |= __ldcg(F + __ldg(a.ccol + k));
+                        if ((acc & miss) == miss) {
+                            ++k;
+                            break;
+                        }
+                    }
+                    edges += k - b;
+                    if (acc & miss) {
+                        a.next[u] = acc & miss;
+                        a.touched[atomicAdd(&n->middle_count, 1u)] = u;
+                    }
+                }
+                uint32_t m = __ballot_sync(dev::kFullMask, mid);
+                while (m) {
+                    const uint32_t j = __ffs(m) - 1;
+                    m &= m - 1;
+                    const uint32_t uj = __shfl_sync(dev::kFullMask, u, j);
+                    const uint32_t bj = __shfl_sync(dev::kFullMask, b, j), dj = __shfl_sync(dev::kFullMask, deg, j);
+                    const unsigned long long mj = __shfl_sync(dev::kFullMask, miss, j);
+                    unsigned long long acc = 0;
+                    uint32_t scanned = 0;
+                    for (uint32_t off = 0; off < dj; off += 32) {
+                        if (off + lane < dj) acc |= __ldcg(F + __ldg(a.ccol + bj + off + lane));
+                        scanned = min(dj, off + 32);
+                        acc = warp_or(acc);
+                        if ((acc & mj) == mj) break;
+                    }
+                    if (lane == 0) {
+                        edges += scanned;
+                        if (acc & mj) {
+                            a.next[uj] = acc & mj;
+                            a.touched[atomicAdd(&n->middle_count, 1u)] = uj;
+                        }
+                    }
+                }
+            }
+            for (uint32_t ch = gw; ch < n_ch; ch += nw) {
+                const uint4 c4 = chunks[ch];
+                const unsigned long long miss = a.full & ~__ldcg(a.seen + c4.x);
+                if (!miss) continue;
+                unsigned long long acc = 0;
+                uint32_t scanned = 0;
+                for (uint32_t off = 0; off < c4.z; off += 32) {
+                    if (off + lane < c4.z) acc |= __ldcg(F + __ldg(a.ccol + c4.y + off + lane));
+                    scanned = min(c4.z, off + 32);
+                    acc = warp_or(acc);
+                    if ((acc & miss) == miss) break;
+                }
+                if (lane == 0) {
+                    edges += scanned;
+                    if (acc & miss) {
+                        const unsigned long long old = atomicOr(a.next + c4.x, acc & miss);
+                        if (old == 0) a.touched[atomicAdd(&n->middle_count, 1u)] = c4.x;
+                    }
                 }
             }
         }
@@ -305,6 +394,12 @@ sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint3
     SG_TRY_CUDA(ctx, ws.get("q1", nv, &a.active[1]));
     SG_TRY_CUDA(ctx, ws.get("middle", nv, &a.touched));
     SG_TRY_CUDA(ctx, ws.get("ctrl", 1, &a.ctrl));
+    // at most sum over split vertices of (deg / kMsChunk + 1) <= 2 * E / kMsChunk chunks per direction
+    a.chunk_cap = (uint32_t)std::min<uint64_t>(2 * (g->ne / kMsChunk) + 2, 0xffffffffu);
+    SG_TRY_CUDA(ctx, ws.get("ms_chunks_out", a.chunk_cap, &a.chunks[0]));
+    SG_TRY_CUDA(ctx, ws.get("ms_chunks_in", a.chunk_cap, &a.chunks[1]));
+    SG_TRY_CUDA(ctx, ws.get("ms_n_chunks", 2, &a.n_chunks));
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(a.n_chunks, 0, 2 * sizeof(uint32_t), ctx->stream));
     uint32_t *dsrc = nullptr;
     SG_TRY_CUDA(ctx, ws.get("ms_sources", 64, &dsrc));
     SG_TRY_CUDA(ctx, cudaMemcpyAsync(dsrc, sources, 4 * nsrc, cudaMemcpyHostToDevice, ctx->stream));

@@ -703,6 +703,9 @@ struct EngineKernel {
     // Local lookahead: the block processes the vertices it discovered itself,
     // up to local_depth levels deep, without waiting for the round's barrier
     // (reorder-safe functors: any order of pushes reaches the same result).
+    // Only under a forced ASYNC_PUSH_DD: the worklist it leaves mixes levels,
+    // and a pull round that takes the first frontier neighbour's offer and
+    // stops (BFS, pull_functor.h:138-188) would keep a level that is too high.
     // Heavy vertices are left to the worklist uncombined, so that a later round
     // splits them into chunks; whatever is still queued at the end goes to the
     // worklist too.  Every thread of the block must call.
@@ -1247,7 +1250,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
             case V_ASYNC_PUSH_DD: {
                 K::clear_dirty(a, s);
                 LocalQ *lq = nullptr;
-                if (a.p.local_depth > 0 && reorder_safe(app)) {
+                if (a.p.local_depth > 0 && a.p.forced == V_ASYNC_PUSH_DD && reorder_safe(app)) {
                     if (threadIdx.x == 0) {
                         lq_block.out = 0;
                         lq_block.n[0] = lq_block.n[1] = 0;
