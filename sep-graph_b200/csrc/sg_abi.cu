@@ -31,6 +31,31 @@ struct DeviceGuard {
     }
 };
 
+// Checks an uploaded CSR (offsets start at 0, end at ne and never decrease;
+// every index < nv) and sums the weights, so that a graph whose edges need no
+// host-side work never goes through a host loop.
+struct CsrCheck {
+    uint32_t ends_bad, first_bad_offset;
+    unsigned long long first_bad_edge;
+    double weight_sum;  // exact: at most 2^32 weights below 2^32
+};
+
+__global__ void validate_csr_kernel(const uint32_t *row, const uint32_t *col, const uint32_t *w, uint32_t nv,
+                                    unsigned long long ne, CsrCheck *chk) {
+    const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+    const unsigned long long nt = (unsigned long long)gridDim.x * blockDim.x;
+    if (tid == 0 && (row[0] != 0 || row[nv] != ne)) chk->ends_bad = 1;
+    for (unsigned long long v = tid; v < nv; v += nt)
+        if (__ldg(row + v + 1) < __ldg(row + v)) atomicMin(&chk->first_bad_offset, (uint32_t)v);
+    double sum = 0;
+    for (unsigned long long e = tid; e < ne; e += nt) {
+        if (__ldg(col + e) >= nv) atomicMin(&chk->first_bad_edge, e);
+        if (w) sum += __ldg(w + e);
+    }
+    sum = dev::warp_sum(sum);
+    if (w && dev::lane_id() == 0 && sum != 0) atomicAdd(&chk->weight_sum, sum);
+}
+
 // Sum of out-degrees and count of vertices whose value differs from `unreached`
 // (GTEPS numerator over the reached component), plus the maximum finite value.
 __global__ void reached_stats_kernel(const uint32_t *row, const uint32_t *value, uint32_t nv, uint32_t unreached,
@@ -269,12 +294,94 @@ sg_status sg_options_default(sg_options *opt) {
     return SG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// A graph whose edges need no host-side work (no CSC to build, or a symmetric
+// unweighted one whose CSC aliases the CSR) is uploaded as it is and checked
+// on the device: host or device inputs, one copy each, one validation kernel.
+sg_status create_on_device(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
+                           const uint32_t *weights, uint32_t flags, sg_graph **out) {
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t b_row = al(4ull * (nv + 1)), b_col = al(4ull * std::max<uint64_t>(ne, 1));
+    const size_t b_w = weights ? b_col : 0;
+    const size_t total = b_row + b_col + b_w + al(sizeof(CsrCheck));
+    sg_graph *g = new (std::nothrow) sg_graph;
+    if (!g) return SG_ERR_OUT_OF_MEMORY;
+    g->ctx = ctx;
+    g->nv = nv;
+    g->ne = ne;
+    g->weighted = weights != nullptr;
+    g->symmetric = flags & SG_GRAPH_SYMMETRIC;
+    g->has_csc = !(flags & SG_GRAPH_NO_CSC);
+    cudaError_t e = cudaMalloc(&g->arena, total);
+    if (e != cudaSuccess) {
+        delete g;
+        return sgb::cuda_status(ctx, e, "graph arena");
+    }
+    g->arena_bytes = total;
+    char *p = (char *)g->arena;
+    g->row = (uint32_t *)p;
+    p += b_row;
+    g->col = (uint32_t *)p;
+    p += b_col;
+    if (weights) {
+        g->w = (uint32_t *)p;
+        p += b_w;
+    }
+    CsrCheck *dchk = (CsrCheck *)p;
+    if (g->has_csc) {  // symmetric: CSC aliases CSR (csr_graph.h:405-410)
+        g->crow = g->row;
+        g->ccol = g->col;
+        g->cw = g->w;
+    }
+    const cudaStream_t s = ctx->stream;
+    CsrCheck hchk{0u, 0xffffffffu, ~0ull, 0.0};
+    uint32_t bad_dst = 0;
+    auto fail = [&](sg_status st) {
+        cudaStreamSynchronize(s);
+        cudaFree(g->arena);
+        delete g;
+        return st;
+    };
+    e = cudaMemcpyAsync(g->row, offsets, 4ull * (nv + 1), cudaMemcpyDefault, s);
+    if (e == cudaSuccess && ne) e = cudaMemcpyAsync(g->col, indices, 4ull * ne, cudaMemcpyDefault, s);
+    if (e == cudaSuccess && weights && ne) e = cudaMemcpyAsync(g->w, weights, 4ull * ne, cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dchk, &hchk, sizeof hchk, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return fail(sgb::cuda_status(ctx, e, "graph upload"));
+    const uint64_t work = std::max<uint64_t>(nv, ne);
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, 148ull * 16));
+    validate_csr_kernel<<<blocks, 256, 0, s>>>(g->row, g->col, g->w, nv, ne, dchk);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hchk, dchk, sizeof hchk, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(sgb::cuda_status(ctx, e, "graph check"));
+    if (hchk.ends_bad) return fail(set_error(ctx, SG_ERR_INVALID_ARG, "offsets[0] must be 0 and offsets[nv] == ne"));
+    if (hchk.first_bad_offset != 0xffffffffu)
+        return fail(set_error(ctx, SG_ERR_INVALID_ARG, "offsets not monotone at %u", hchk.first_bad_offset));
+    if (hchk.first_bad_edge != ~0ull) {
+        cudaMemcpy(&bad_dst, g->col + hchk.first_bad_edge, 4, cudaMemcpyDeviceToHost);
+        return fail(set_error(ctx, SG_ERR_INVALID_ARG, "edge %llu points to vertex %u >= nv", hchk.first_bad_edge, bad_dst));
+    }
+    g->weight_sum = weights ? hchk.weight_sum : (double)ne;
+    ctx->live_graphs++;
+    *out = g;
+    return SG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
                           const uint32_t *weights, uint32_t flags, sg_graph **out) {
     if (!ctx || !out || !offsets || (ne && !indices) || nv == 0) return SG_ERR_INVALID_ARG;
     if (ne >= (1ull << 32)) return set_error(ctx, SG_ERR_INVALID_ARG, "edge count %llu exceeds uint32", (unsigned long long)ne);
     *out = nullptr;
     DeviceGuard dg(ctx->device);
+    if ((flags & SG_GRAPH_NO_CSC) || ((flags & SG_GRAPH_SYMMETRIC) && !weights))
+        return create_on_device(ctx, nv, ne, offsets, indices, weights, flags, out);
     // Inputs may be host or device memory; validation and the CSC build run on host copies.
     const bool dev_in = sgb::is_device_ptr(offsets, ctx->device);
     std::vector<uint32_t> h_off, h_idx, h_w;

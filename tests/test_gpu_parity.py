@@ -210,3 +210,34 @@ def test_repeat_runs_deterministic(ctx):
     G = ctx.graph(h)
     outs = [G.sssp(int(h.pick_sources(1, 1)[0]))[0] for _ in range(3)]
     assert all((o == outs[0]).all() for o in outs)
+
+
+@pytest.mark.parametrize("no_csc", [False, True])
+def test_invalid_csr_rejected(ctx, no_csc):
+    """Malformed CSR is rejected both by the host check (graphs that build a
+    CSC on the host) and by the device check (graphs uploaded as they are)."""
+    good_off = np.array([0, 2, 3, 3], np.uint32)
+    good_idx = np.array([1, 2, 0], np.uint32)
+    for off, idx in ((np.array([1, 2, 3, 3], np.uint32), good_idx),      # does not start at 0
+                     (np.array([0, 2, 1, 3], np.uint32), good_idx),      # not monotone
+                     (good_off, np.array([1, 3, 0], np.uint32))):        # index out of range
+        with pytest.raises(sg.SGError) as e:
+            ctx.graph_from_csr(off, idx, no_csc=no_csc)
+        assert e.value.status == 1
+    G = ctx.graph_from_csr(good_off, good_idx, no_csc=no_csc)  # the context is still usable
+    assert (G.bfs(0)[0] == np.array([0, 1, 2], np.uint32)).all()
+
+
+def test_device_checked_upload_matches_host_path(ctx):
+    torch = pytest.importorskip("torch")
+    h = sg.HostGraph.rmat(13, 16, seed=3).gen_weights(1, 64, 4)
+    off = torch.from_numpy(h.offsets.astype(np.int32)).cuda()
+    idx = torch.from_numpy(h.indices.astype(np.int32)).cuda()
+    w = torch.from_numpy(h.weights.astype(np.int32)).cuda()
+    Gd = ctx.graph_from_csr(off, idx, w, no_csc=True)    # device inputs, device check
+    Gh = ctx.graph(h)                                      # host inputs, host check + CSC
+    for s in (int(x) for x in h.pick_sources(3, 5)):
+        # default two-level delta comes from the weight sum each path computed
+        a, _, _ = Gd.sssp(s, priority="low_high", max_iteration=1000000)
+        b, _, _ = Gh.sssp(s, priority="low_high", max_iteration=1000000)
+        assert (a == b).all() and (a == oracle.sssp(h.offsets, h.indices, h.weights, s)).all()
