@@ -7,9 +7,9 @@
 // for other slots to release memory when it does not fit), runs them as one
 // batched launch and completes their tickets.  Requests that arrive while a
 // batch runs are taken by the next free slot, so work from different batches
-// overlaps on the device.  PageRank (and BC with path counts) run through the
-// graph's own context, serialised per context: a caller must not use that
-// context itself while queries on its graphs are in flight.
+// overlaps on the device.  PageRank (and BC with path counts) run as single
+// queries on a view of the graph bound to the slot's own context, so they
+// never share a stream or scratch with another slot or with the caller.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -34,7 +34,6 @@ struct GraphInfo {
     sg_graph *g;
     uint32_t nv;
     uint64_t ne;
-    std::mutex *ctx_mu;  // serialises single-query calls on the graph's own context (stream, scratch)
 };
 
 // The graph table never reallocates, so workers index it without the lock
@@ -59,7 +58,9 @@ struct sg_server {
     int device = 0;
     sg_server_config cfg{};
     std::vector<GraphInfo> graphs;
-    std::map<sg_ctx *, std::unique_ptr<std::mutex>> ctx_locks;
+    // views[slot][graph]: the graph bound to the slot's context with its own
+    // workspace, made on first use by that slot's worker only
+    std::vector<std::vector<sg_graph *>> views;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Pending> pending;
@@ -76,6 +77,7 @@ struct sg_server {
     Clock::time_point t_first, t_last;
 
     void worker(int slot);
+    sg_graph *view(int slot, uint32_t graph_id);
     void run_batch(int slot, std::vector<Pending> &batch, std::vector<sg_status> &status);
     uint64_t estimate(const std::vector<Pending> &b) const;
 };
@@ -119,6 +121,13 @@ void run_isolated(const std::vector<sg_batch_query> &q, const std::vector<size_t
 }
 
 }  // namespace
+
+sg_graph *sg_server::view(int slot, uint32_t graph_id) {
+    std::vector<sg_graph *> &v = views[slot];
+    if (v.size() <= graph_id) v.resize(graph_id + 1, nullptr);
+    if (!v[graph_id]) v[graph_id] = sgb::graph_view(graphs[graph_id].g, slot_ctx[slot]);
+    return v[graph_id];
+}
 
 uint64_t sg_server::estimate(const std::vector<Pending> &b) const {
     // Device scratch of one batch: per-team workspaces sized for the largest
@@ -197,11 +206,8 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
         for (auto &kv : by_graph) {
             GraphInfo &gi = graphs[kv.first];
             std::vector<float> ranks(gi.nv);
-            sg_status st;
-            {
-                std::lock_guard<std::mutex> lk(*gi.ctx_mu);
-                st = sg_pagerank(gi.g, &o, ranks.data(), nullptr, nullptr);
-            }
+            sg_graph *gv = view(slot, kv.first);
+            const sg_status st = gv ? sg_pagerank(gv, &o, ranks.data(), nullptr, nullptr) : SG_ERR_OUT_OF_MEMORY;
             for (size_t i : kv.second) {
                 status[i] = st;
                 if (st == SG_OK) std::memcpy(b[i].q.out, ranks.data(), 4ull * gi.nv);
@@ -214,9 +220,9 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
         std::vector<size_t> in_batch;
         for (size_t i = 0; i < b.size(); ++i) {
             if (b[i].q.out2) {
-                GraphInfo &gi = graphs[b[i].q.graph_id];
-                std::lock_guard<std::mutex> lk(*gi.ctx_mu);  // sg_bc runs on the graph's own context
-                status[i] = sg_bc(gi.g, b[i].q.source, &o, (float *)b[i].q.out, (uint64_t *)b[i].q.out2, nullptr);
+                sg_graph *gv = view(slot, b[i].q.graph_id);
+                status[i] = gv ? sg_bc(gv, b[i].q.source, &o, (float *)b[i].q.out, (uint64_t *)b[i].q.out2, nullptr)
+                               : SG_ERR_OUT_OF_MEMORY;
             } else {
                 q.push_back({graphs[b[i].q.graph_id].g, b[i].q.source, 0, b[i].q.out});
                 in_batch.push_back(i);
@@ -322,6 +328,7 @@ sg_status sg_server_create(int device, const sg_server_config *cfg, sg_server **
     uint64_t hbm = 0;
     sg_device_info(s->slot_ctx[0], nullptr, &hbm, nullptr, nullptr, 0);
     s->budget = s->cfg.hbm_budget_bytes ? s->cfg.hbm_budget_bytes : hbm / 4;
+    s->views.resize(s->cfg.slots);
     sg_server *raw = s.release();
     for (uint32_t k = 0; k < raw->cfg.slots; ++k) raw->workers.emplace_back([raw, k] { raw->worker((int)k); });
     *out = raw;
@@ -334,12 +341,9 @@ sg_status sg_server_add_graph(sg_server *s, sg_graph *g, uint32_t *graph_id) {
     uint64_t ne = 0;
     sg_status st = sg_graph_info(g, &nv, &ne, nullptr, nullptr);
     if (st != SG_OK) return st;
-    sg_ctx *owner = sgb::graph_context(g);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->graphs.size() >= kMaxGraphs) return SG_ERR_BUSY;
-    auto &m = s->ctx_locks[owner];
-    if (!m) m = std::make_unique<std::mutex>();
-    s->graphs.push_back({g, nv, ne, m.get()});
+    s->graphs.push_back({g, nv, ne});
     *graph_id = (uint32_t)s->graphs.size() - 1;
     return SG_OK;
 }
@@ -438,6 +442,8 @@ sg_status sg_server_destroy(sg_server *s) {
     s->cv_work.notify_all();
     s->cv_done.notify_all();
     for (auto &t : s->workers) t.join();
+    for (auto &per_slot : s->views)
+        for (sg_graph *v : per_slot) sgb::graph_view_destroy(v);
     for (auto *c : s->slot_ctx) sg_destroy(c);
     delete s;
     return SG_OK;

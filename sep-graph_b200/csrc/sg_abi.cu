@@ -520,6 +520,34 @@ sg_status sg_graph_destroy(sg_graph *g) {
 sg_ctx *sgb::graph_context(const sg_graph *g) { return g ? g->ctx : nullptr; }
 double sgb::graph_weight_sum(const sg_graph *g) { return g ? g->weight_sum : 0.0; }
 
+sg_graph *sgb::graph_view(sg_graph *g, sg_ctx *ctx) {
+    if (!g || !ctx || g->ctx->device != ctx->device) return nullptr;
+    sg_graph *v = new (std::nothrow) sg_graph;
+    if (!v) return nullptr;
+    v->ctx = ctx;
+    v->nv = g->nv;
+    v->ne = g->ne;
+    v->weighted = g->weighted;
+    v->symmetric = g->symmetric;
+    v->has_csc = g->has_csc;
+    v->weight_sum = g->weight_sum;
+    v->arena = nullptr;  // the arrays stay owned by g
+    v->row = g->row;
+    v->col = g->col;
+    v->w = g->w;
+    v->crow = g->crow;
+    v->ccol = g->ccol;
+    v->cw = g->cw;
+    return v;
+}
+
+void sgb::graph_view_destroy(sg_graph *view) {
+    if (!view) return;
+    DeviceGuard dg(view->ctx->device);
+    cudaStreamSynchronize(view->ctx->stream);
+    delete view;  // frees the view's own workspace only
+}
+
 extern "C" {
 
 sg_status sg_graph_info(const sg_graph *g, uint32_t *nv, uint64_t *ne, uint64_t *device_bytes, int *weighted) {
