@@ -63,6 +63,7 @@ def args_parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--quick", action="store_true", help="headline line only")
     p.add_argument("--served-queries", type=int, default=1000)
+    p.add_argument("--extras", default="per_algo,batched,served", help="extra sections at N=1 (comma list)")
     p.add_argument("--scale", type=int, default=SCALE)
     p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc"],
                    help="run one warm-up and one measured solve of that kernel only (for ncu captures)")
@@ -371,7 +372,10 @@ def run_ours(a):
     if world == 1 and not a.quick:
         extra = {}
         cache = {"rmat22": (h, G)}
+        wanted = set(a.extras.split(","))
         for name, fn in (("per_algo", per_algo), ("batched", batched), ("served", served)):
+            if name not in wanted:
+                continue
             t0 = time.perf_counter()
             try:
                 extra[name] = fn(ctx, cache, a)
@@ -392,7 +396,7 @@ def run_ours(a):
 
 def read_traffic(mode):
     """DRAM bytes per launch of the engine kernel from the committed ncu summary of the selected mode."""
-    name = "sssp_rmat22_delta_engine_kernel.md" if mode.startswith("delta") else "sssp_rmat22_push_dd_engine_kernel.md"
+    name = "sssp_rmat21_delta_engine_kernel.md" if mode.startswith("delta") else "sssp_rmat22_push_dd_engine_kernel.md"
     try:
         for line in open(os.path.join(ROOT, "profiles", name)):
             if line.startswith("dram_bytes_per_launch_full_size:"):

@@ -275,6 +275,9 @@ sg_status sg_server_drain(sg_server *s, double timeout_s);
 sg_status sg_server_get_stats(sg_server *s, sg_server_stats *st);
 sg_status sg_server_reset_stats(sg_server *s);
 sg_status sg_server_destroy(sg_server *s);
+/* With the environment variable SEPGRAPH_SERVER_LOG naming a file when the
+ * server is created, every batch appends one line to it: slot, algorithm,
+ * queries, estimated device bytes, device-side wall time in ms. */
 
 /* ------------------------------------------------------------------ autotuner
  * No counterpart in the reference (its variants, thresholds and grid shape are

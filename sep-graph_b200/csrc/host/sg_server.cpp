@@ -14,6 +14,8 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -74,6 +76,9 @@ struct sg_server {
     uint64_t submitted = 0, completed = 0, failed = 0, batches = 0;
     std::vector<double> latencies;
     bool have_first = false;
+    // optional batch log (one line per batch) when SEPGRAPH_SERVER_LOG names a file
+    FILE *log = nullptr;
+    std::mutex log_mu;
     Clock::time_point t_first, t_last;
 
     void worker(int slot);
@@ -268,8 +273,16 @@ void sg_server::worker(int slot) {
             if (!pending.empty()) cv_work.notify_one();
         }
         std::vector<sg_status> status;
+        const auto t_run = Clock::now();
         run_batch(slot, batch, status);
         const auto now = Clock::now();
+        if (log) {
+            std::lock_guard<std::mutex> lk(log_mu);
+            std::fprintf(log, "slot %d algo %d queries %zu est_bytes %llu ms %.3f\n", slot, batch.front().q.algo,
+                         batch.size(), (unsigned long long)est,
+                         std::chrono::duration<double, std::milli>(now - t_run).count());
+            std::fflush(log);
+        }
         {
             std::lock_guard<std::mutex> lk(mu);
             in_use -= est;
@@ -329,6 +342,7 @@ sg_status sg_server_create(int device, const sg_server_config *cfg, sg_server **
     sg_device_info(s->slot_ctx[0], nullptr, &hbm, nullptr, nullptr, 0);
     s->budget = s->cfg.hbm_budget_bytes ? s->cfg.hbm_budget_bytes : hbm / 4;
     s->views.resize(s->cfg.slots);
+    if (const char *path = std::getenv("SEPGRAPH_SERVER_LOG")) s->log = std::fopen(path, "a");
     sg_server *raw = s.release();
     for (uint32_t k = 0; k < raw->cfg.slots; ++k) raw->workers.emplace_back([raw, k] { raw->worker((int)k); });
     *out = raw;
@@ -445,6 +459,7 @@ sg_status sg_server_destroy(sg_server *s) {
     for (auto &per_slot : s->views)
         for (sg_graph *v : per_slot) sgb::graph_view_destroy(v);
     for (auto *c : s->slot_ctx) sg_destroy(c);
+    if (s->log) std::fclose(s->log);
     delete s;
     return SG_OK;
 }
