@@ -330,12 +330,19 @@ def run_ours(a):
     e2e_kw = dict(kw, blocking=1)
     barrier()
     t0 = time.perf_counter()
+    parts = {"upload_and_check": 0.0, "queries": 0.0, "release": 0.0}
     for _ in range(e2e_steps):
+        ta = time.perf_counter()
         G2 = ctx.graph_from_csr(off_p.data_ptr(), idx_p.data_ptr(), w_p.data_ptr(), nv=nv, ne=ne,
                                 no_csc=tuned["variant"] == "async_push_dd")
+        tb = time.perf_counter()
         for s in srcs:
             G2.sssp(s, out=host_out.numpy(), **e2e_kw)
+        tc = time.perf_counter()
         G2.close()
+        parts["upload_and_check"] += tb - ta
+        parts["queries"] += tc - tb
+        parts["release"] += time.perf_counter() - tc
     ctx.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = sum_over_ranks(step_edges * e2e_steps) / e2e_s / 1e9
@@ -359,7 +366,8 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (graph arrays %.0f MB vs 126 MB L2)" % ((4 * (nv + 1) + 8 * ne) / 1e6),
                    "parallelism": f"replicas{world}"},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "what": "per step: pinned CSR+weights upload, 8 queries into pinned host distance arrays"},
+                "what": "per step: pinned CSR+weights upload, 8 queries into pinned host distance arrays",
+                "ms_per_step": {k: 1e3 * v / e2e_steps for k, v in parts.items()}},
         "gpu_launches": a.steps * len(srcs),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "hybrid_engine_kernel<SSSP>",

@@ -167,7 +167,7 @@ sg_status reached_stats(sg_graph *g, const uint32_t *value, sg_stats *stats) {
     if (!stats) return SG_OK;
     sg_ctx *ctx = g->ctx;
     unsigned long long *d = nullptr;
-    SG_TRY_CUDA(ctx, g->ws.get("reach_stats", 3, &d));
+    SG_TRY_CUDA(ctx, sgb::graph_ws(g).get("reach_stats", 3, &d));
     SG_TRY_CUDA(ctx, cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), ctx->stream));
     const int blocks = std::max(1, std::min<int>((g->nv + 255) / 256, ctx->prop.multiProcessorCount * 8));
     reached_stats_kernel<<<blocks, 256, 0, ctx->stream>>>(g->row, value, g->nv, apps::kInf, d);
@@ -247,6 +247,7 @@ sg_status sg_destroy(sg_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     delete ctx->batch_ws;
+    delete ctx->graph_ws;
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -545,7 +546,7 @@ void sgb::graph_view_destroy(sg_graph *view) {
     if (!view) return;
     DeviceGuard dg(view->ctx->device);
     cudaStreamSynchronize(view->ctx->stream);
-    delete view;  // frees the view's own workspace only
+    delete view;  // the arrays stay with the graph, the scratch with the context
 }
 
 extern "C" {
@@ -554,7 +555,7 @@ sg_status sg_graph_info(const sg_graph *g, uint32_t *nv, uint64_t *ne, uint64_t 
     if (!g) return SG_ERR_INVALID_ARG;
     if (nv) *nv = g->nv;
     if (ne) *ne = g->ne;
-    if (device_bytes) *device_bytes = g->arena_bytes + g->ws.total_bytes();
+    if (device_bytes) *device_bytes = g->arena_bytes;
     if (weighted) *weighted = g->weighted;
     return SG_OK;
 }
@@ -570,8 +571,8 @@ sg_status sg_bfs(sg_graph *g, uint32_t source, const sg_options *opt, uint32_t *
     if (out_dev)
         value = levels_out;
     else
-        SG_TRY_CUDA(ctx, g->ws.get("value_u32", g->nv, &value));
-    SG_TRY_CUDA(ctx, g->ws.get("buffer_u32", g->nv, &buffer));
+        SG_TRY_CUDA(ctx, sgb::graph_ws(g).get("value_u32", g->nv, &value));
+    SG_TRY_CUDA(ctx, sgb::graph_ws(g).get("buffer_u32", g->nv, &buffer));
     // local lookahead mixes levels inside a round, which needs the atomic minimum
     apps::BFS<uint32_t, uint32_t, graphs::NoWeight> app(source, o.non_atomic != 0 && o.local_depth <= 0);
     sgb::EngineResult res;
@@ -608,8 +609,8 @@ sg_status sg_sssp(sg_graph *g, uint32_t source, const sg_options *opt, uint32_t 
     if (out_dev)
         value = dist_out;
     else
-        SG_TRY_CUDA(ctx, g->ws.get("value_u32", g->nv, &value));
-    SG_TRY_CUDA(ctx, g->ws.get("buffer_u32", g->nv, &buffer));
+        SG_TRY_CUDA(ctx, sgb::graph_ws(g).get("value_u32", g->nv, &value));
+    SG_TRY_CUDA(ctx, sgb::graph_ws(g).get("buffer_u32", g->nv, &buffer));
     apps::SSSP<uint32_t, uint32_t, uint32_t> app(source);
     sgb::EngineResult res;
     sg_status st = sgb::run_engine<decltype(app), uint32_t, uint32_t, uint32_t>(g, app, cfg, value, buffer, &res);
@@ -630,11 +631,11 @@ sg_status sg_pagerank(sg_graph *g, const sg_options *opt, float *ranks_out, floa
     if (out_dev)
         value = ranks_out;
     else
-        SG_TRY_CUDA(ctx, g->ws.get("value_f32", g->nv, &value));
+        SG_TRY_CUDA(ctx, sgb::graph_ws(g).get("value_f32", g->nv, &value));
     if (res_dev)
         buffer = residual_out;
     else
-        SG_TRY_CUDA(ctx, g->ws.get("buffer_f32", g->nv, &buffer));
+        SG_TRY_CUDA(ctx, sgb::graph_ws(g).get("buffer_f32", g->nv, &buffer));
     apps::PageRank<float, float, graphs::NoWeight> app(o.pr_error);
     sgb::EngineResult res;
     sg_status st = sgb::run_engine<decltype(app), float, float, graphs::NoWeight>(g, app, cfg, value, buffer, &res);
@@ -667,7 +668,7 @@ sg_status sg_bc(sg_graph *g, uint32_t source, const sg_options *opt, float *bc_o
     float *delta = nullptr, *bcv = nullptr;
     const bool sig_dev = sgb::is_device_ptr(sigma_out, ctx->device);
     const bool bc_dev = sgb::is_device_ptr(bc_out, ctx->device);
-    auto &ws = g->ws;
+    auto &ws = sgb::graph_ws(g);
     SG_TRY_CUDA(ctx, ws.get("value_u32", nv, &level));
     SG_TRY_CUDA(ctx, ws.get("buffer_u32", nv, &buffer));
     SG_TRY_CUDA(ctx, ws.get("bc_stack", nv, &stack));

@@ -17,10 +17,10 @@ sg_status msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint32_t n
 sg_ctx *graph_context(const sg_graph *g);
 // Sum of the graph's edge weights (its edge count when unweighted).
 double graph_weight_sum(const sg_graph *g);
-// A view of g's device arrays bound to another context of the same device,
-// with its own workspace: single-query calls on the view run on that
-// context's stream and never touch g's scratch.  The view must be released
-// with graph_view_destroy before g is destroyed.
+// A view of g's device arrays bound to another context of the same device:
+// single-query calls on the view run on that context's stream with that
+// context's scratch.  The view must be released with graph_view_destroy
+// before g is destroyed.
 sg_graph *graph_view(sg_graph *g, sg_ctx *ctx);
 void graph_view_destroy(sg_graph *view);
 

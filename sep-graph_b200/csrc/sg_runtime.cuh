@@ -35,6 +35,7 @@ struct sg_ctx {
     size_t pinned_bytes = 0;
     int live_graphs = 0;  // sg_destroy refuses while graphs of this context exist
     sgb::Workspace *batch_ws = nullptr;  // scratch of batched launches (team workspaces)
+    sgb::Workspace *graph_ws = nullptr;  // scratch of single-query calls, shared by the context's graphs
 };
 
 namespace sgb {
@@ -92,8 +93,17 @@ struct sg_graph {
     size_t arena_bytes = 0;
     uint32_t *row = nullptr, *col = nullptr, *w = nullptr;
     uint32_t *crow = nullptr, *ccol = nullptr, *cw = nullptr;
-    sgb::Workspace ws;
 };
+
+namespace sgb {
+// Scratch of single-query calls on g: the context's, grow-only and shared by
+// all its graphs (work of a context is ordered on its stream), so creating
+// another graph allocates no new scratch.
+inline Workspace &graph_ws(sg_graph *g) {
+    if (!g->ctx->graph_ws) g->ctx->graph_ws = new Workspace;
+    return *g->ctx->graph_ws;
+}
+}  // namespace sgb
 
 namespace sgb {
 
@@ -228,7 +238,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     const uint32_t chunk_edges = std::max<uint32_t>(32, cfg.chunk_edges);
     const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(nv, ne / heavy_threshold) + 2;
     const uint32_t chunk_cap = (uint32_t)(ne / chunk_edges + heavy_cap + 2);
-    auto &ws = g->ws;
+    auto &ws = sgb::graph_ws(g);
     SG_TRY_CUDA(ctx, ws.get("tmp", nv, &a.tmp));
     SG_TRY_CUDA(ctx, ws.get("q0", nv, &a.queue[0]));
     SG_TRY_CUDA(ctx, ws.get("q1", nv, &a.queue[1]));
@@ -363,7 +373,7 @@ class Engine {
 
     sg_status Start() {
         if (!m_graph || !m_app) return SG_ERR_INVALID_ARG;
-        auto &ws = m_graph->ws;
+        auto &ws = sgb::graph_ws(m_graph);
         if (ws.get("engine_value", m_graph->nv, &m_value) != cudaSuccess ||
             ws.get("engine_buffer", m_graph->nv, &m_buffer) != cudaSuccess)
             return SG_ERR_OUT_OF_MEMORY;
