@@ -99,6 +99,7 @@ sg_options server_options(const sg_server_config &c, int algo) {
         // each graph's own reference heuristic 32*avg_w/avg_deg when it is 0
         o.priority = SG_PRIORITY_LOW_HIGH;
         o.priority_delta = c.sssp_delta;
+        o.local_depth = 16;  // blocks follow their own discoveries inside a round (bit-exact, fewer rounds)
     }
     if (algo == SG_QUERY_PAGERANK) {
         o.pr_error = c.pr_error;

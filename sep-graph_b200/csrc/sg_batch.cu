@@ -56,7 +56,7 @@ struct MsArgs {
     uint32_t *n_chunks;  // [2], zero at launch
     Ctrl *ctrl;
     uint32_t max_rounds;
-    double alpha;
+    double alpha, beta;
     long long total_edges;
     unsigned long long timeout_ns;
     int force_dir;  // -1 auto, 0 push, 1 pull
@@ -272,19 +272,22 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
             const uint32_t *act = a.active[cur];
             for (uint32_t i = gthread(); i < s.F; i += nthreads()) a.fr[cur][__ldcg(act + i)] = 0;
             const uint32_t T = __ldcg(&n->middle_count);
-            unsigned long long scout = 0;
+            unsigned long long scout = 0, explored = 0;
             for (uint32_t base = gw * 32; base < T; base += nw * 32) {
                 const uint32_t i = base + lane;
                 uint32_t u = 0;
                 unsigned long long nb = 0;
                 if (i < T) {
-                    u = __ldcg(a.touched + i);
-                    nb = __ldcg(a.next + u) & ~__ldcg(a.seen + u);
+                    u = __ldcg(a.touched + i);  // listed once per round
+                    const unsigned long long was = __ldcg(a.seen + u);
+                    nb = __ldcg(a.next + u) & ~was;
                     a.next[u] = 0;
                     if (nb) {
-                        a.seen[u] |= nb;
+                        a.seen[u] = was | nb;
                         a.fr[nxt][u] = nb;
-                        scout += __ldg(a.row + u + 1) - __ldg(a.row + u);
+                        const uint32_t deg = __ldg(a.row + u + 1) - __ldg(a.row + u);
+                        scout += deg;
+                        if (!was) explored += deg;  // first source to reach u: its edges leave the unexplored set
                         for (unsigned long long m = nb; m; m &= m - 1)
                             a.levels[(uint64_t)(__ffsll(m) - 1) * a.nv + u] = s.round;
                     }
@@ -292,24 +295,31 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
                 dev::warp_append(a.active[nxt], &n->qcount[nxt], a.nv, nb != 0, u, &n->error);
             }
             scout = dev::warp_sum(scout);
+            explored = dev::warp_sum(explored);
             if (lane == 0 && scout) atomicAdd(&n->scout[nxt], scout);
+            if (lane == 0 && explored) atomicAdd(&n->scout[2], explored);
         }
         auto end_round = [&] {
             const uint32_t F2 = dev::ld_l2(&n->qcount[nxt]);
             const unsigned long long sc = dev::ld_l2(&n->scout[nxt]);
-            if (ps.rs.variant == 0) ++L.rounds_push; else ++L.rounds_pull;
-            L.unexplored -= (long long)sc;
+            const unsigned long long ex = dev::ld_l2(&n->scout[2]);
+            const bool was_pull = ps.rs.variant == 1;
+            if (was_pull) ++L.rounds_pull; else ++L.rounds_push;
+            L.unexplored -= (long long)ex;
             if (L.unexplored < 0) L.unexplored = 0;
             n->qcount[cur] = 0;
             n->scout[cur] = 0;
+            n->scout[2] = 0;
             n->middle_count = 0;
             ps.rs.qin = nxt;
             ps.rs.F = F2;
             ps.rs.round++;
             if (a.force_dir >= 0)
                 ps.rs.variant = a.force_dir;
-            else
-                ps.rs.variant = (double)sc > (double)L.unexplored / a.alpha ? 1 : 0;
+            else  // the engine's traversal rule (hybrid_policy.h:265-288): stay in pull while the
+                  // frontier is large, switch to pull when its edges outweigh the unexplored ones
+                ps.rs.variant = ((was_pull && (double)F2 > (double)a.nv / a.beta) ||
+                                 (double)sc > (double)L.unexplored / a.alpha) ? 1 : 0;
             if (F2 == 0 || ps.rs.round > a.max_rounds) {
                 ps.rs.done = 1;
                 c->round = ps.rs.round - 1;
@@ -411,6 +421,7 @@ sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint3
         SG_TRY_CUDA(ctx, ws.get("ms_levels", (size_t)nsrc * nv, &a.levels));
     a.max_rounds = o.max_iteration > 0 ? (uint32_t)o.max_iteration : 200u;
     a.alpha = o.alpha > 0 ? o.alpha : 15;
+    a.beta = o.beta > 0 ? o.beta : 18;
     a.total_edges = (long long)g->ne;
     a.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
     a.force_dir = o.variant == SG_ASYNC_PUSH_DD ? 0 : (o.variant == SG_ASYNC_PULL_DD ? 1 : -1);
