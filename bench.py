@@ -546,6 +546,22 @@ def batched(ctx, cache, a):
         "msbfs_ms": ms_m, "msbfs_qps": 64 / (ms_m * 1e-3), "msbfs_GTEPS": e / ms_m / 1e6, "msbfs_same_results": same_m}
     del plain, outs, lv_m
 
+    # the same on a high-diameter graph: 16 sources on the 4096x4096 grid
+    hg = sg.HostGraph.grid(4096, 4096)
+    Gg = ctx.graph(hg)
+    gsrcs = [int(x) for x in hg.pick_sources(16, 12)]
+    plain_g, plain_ms_g = [], 0.0
+    for s_ in gsrcs:
+        lv, st, _ = Gg.bfs(s_, max_iteration=1000000)
+        plain_ms_g += st.time_kernel_ms
+        plain_g.append(lv)
+    ms_g, (lv_g, _) = _median_ms(lambda: Gg.msbfs(gsrcs, max_iteration=1000000), 3)
+    res["bfs16_grid4096"] = {"plain_ms": plain_ms_g, "plain_qps": 16 / (plain_ms_g * 1e-3), "msbfs_ms": ms_g,
+                             "msbfs_qps": 16 / (ms_g * 1e-3),
+                             "msbfs_same_results": all((lv_g[i] == plain_g[i]).all() for i in range(16))}
+    Gg.close()
+    del hg, plain_g, lv_g
+
     srcs32 = srcs[:32]
     plain_ms, plain = 0.0, []
     for s in srcs32:

@@ -11,7 +11,8 @@
 // by degree: a thread per vertex up to 32 edges, a warp per vertex up to 2048,
 // and 2048-edge chunks of bigger vertices (listed once per launch) spread over
 // all warps, so one hub never holds up a round.  The direction switch uses the
-// single-source engine's rule (scout count against unexplored edges / alpha,
+// single-source engine's rule (scout count against the in-edges of vertices
+// some source has not reached yet / alpha, and beta for leaving pull,
 // include/framework/hybrid_policy.h:265-288).  No reference counterpart: the
 // reference runs one source per Engine.
 #include <cuda_runtime.h>
@@ -285,9 +286,9 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
                     if (nb) {
                         a.seen[u] = was | nb;
                         a.fr[nxt][u] = nb;
-                        const uint32_t deg = __ldg(a.row + u + 1) - __ldg(a.row + u);
-                        scout += deg;
-                        if (!was) explored += deg;  // first source to reach u: its edges leave the unexplored set
+                        scout += __ldg(a.row + u + 1) - __ldg(a.row + u);
+                        // u now seen by every source: a pull round no longer scans its in-edges
+                        if ((was | nb) == a.full) explored += __ldg(a.crow + u + 1) - __ldg(a.crow + u);
                         for (unsigned long long m = nb; m; m &= m - 1)
                             a.levels[(uint64_t)(__ffsll(m) - 1) * a.nv + u] = s.round;
                     }
@@ -317,7 +318,8 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
             if (a.force_dir >= 0)
                 ps.rs.variant = a.force_dir;
             else  // the engine's traversal rule (hybrid_policy.h:265-288): stay in pull while the
-                  // frontier is large, switch to pull when its edges outweigh the unexplored ones
+                  // frontier is large, switch to pull when its edges outweigh the edges a pull
+                  // round would scan (in-edges of the vertices some source has not reached)
                 ps.rs.variant = ((was_pull && (double)F2 > (double)a.nv / a.beta) ||
                                  (double)sc > (double)L.unexplored / a.alpha) ? 1 : 0;
             if (F2 == 0 || ps.rs.round > a.max_rounds) {

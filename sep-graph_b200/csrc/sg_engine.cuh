@@ -896,24 +896,42 @@ struct EngineKernel {
                 w.beg[lane] = beg;
                 w.pay[lane] = app.PullIdentity();
                 __syncwarp();
-                for (uint32_t eb = 0; eb < total; eb += 32) {
-                    const uint32_t e = eb + lane;
-                    uint32_t k = 0xffffffffu;
-                    TB x = app.PullIdentity();
-                    if (e < total) {
-                        k = owner(w.excl, e);
-                        x = dev::ld_l2(srcbuf + a.csc.edge_src(w.beg[k] + (e - w.excl[k])));
-                    }
-                    // segmented reduction: lanes of one destination are contiguous
+                // four 32-edge batches per step: their index loads, then their
+                // gathers, are issued together (four times the loads in flight
+                // of one batch at a time), then reduced one batch after another
+                constexpr int kUnroll = 4;
+                for (uint32_t eb = 0; eb < total; eb += 32 * kUnroll) {
+                    uint32_t k[kUnroll], src[kUnroll];
+                    TB x[kUnroll];
 #pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const TB y = __shfl_down_sync(dev::kFullMask, x, d);
-                        const uint32_t ky = __shfl_down_sync(dev::kFullMask, k, d);
-                        if (lane + d < 32 && ky == k) x = app.PullReduce(x, y);
+                    for (int j = 0; j < kUnroll; ++j) {
+                        const uint32_t e = eb + 32 * j + lane;
+                        k[j] = 0xffffffffu;
+                        src[j] = 0;
+                        if (e < total) {
+                            k[j] = owner(w.excl, e);
+                            src[j] = a.csc.edge_src(w.beg[k[j]] + (e - w.excl[k[j]]));
+                        }
                     }
-                    const uint32_t kp = __shfl_up_sync(dev::kFullMask, k, 1);
-                    if (e < total && (lane == 0 || kp != k)) w.pay[k] = app.PullReduce(w.pay[k], x);
-                    __syncwarp();
+#pragma unroll
+                    for (int j = 0; j < kUnroll; ++j)
+                        x[j] = k[j] != 0xffffffffu ? dev::ld_l2(srcbuf + src[j]) : app.PullIdentity();
+#pragma unroll
+                    for (int j = 0; j < kUnroll; ++j) {
+                        if (eb + 32 * j >= total) break;  // the same in every lane
+                        // segmented reduction: lanes of one destination are contiguous
+                        TB xj = x[j];
+                        const uint32_t kj = k[j];
+#pragma unroll
+                        for (int d = 1; d < 32; d <<= 1) {
+                            const TB y = __shfl_down_sync(dev::kFullMask, xj, d);
+                            const uint32_t ky = __shfl_down_sync(dev::kFullMask, kj, d);
+                            if (lane + d < 32 && ky == kj) xj = app.PullReduce(xj, y);
+                        }
+                        const uint32_t kp = __shfl_up_sync(dev::kFullMask, kj, 1);
+                        if (kj != 0xffffffffu && (lane == 0 || kp != kj)) w.pay[kj] = app.PullReduce(w.pay[kj], xj);
+                        __syncwarp();
+                    }
                 }
                 __syncwarp();
                 if (v < N && deg > 0) accumulate<App, TB, TW>(app, a.csc_w, v, v, beg, a.buffer + v, w.pay[lane]);
