@@ -249,11 +249,26 @@ void sg_server::worker(int slot) {
             std::unique_lock<std::mutex> lk(mu);
             cv_work.wait(lk, [&] { return stop || !pending.empty(); });
             if (stop && pending.empty()) return;
-            // the oldest request decides the algorithm; take its peers in arrival order
+            // the oldest request decides the algorithm; take its peers in arrival order.
+            // BFS on a graph with enough pending queries is one multi-source launch of
+            // that graph alone (up to 64 sources), and PageRank is one run per graph
+            // for all its pending queries, so that other slots run the other graphs'
+            // launches at the same time.
             const int algo = pending.front().q.algo;
-            const uint32_t cap = cfg.max_batch;
+            const uint32_t graph = pending.front().q.graph_id;
+            uint32_t cap = cfg.max_batch;
+            bool one_graph = algo == SG_QUERY_PAGERANK;
+            if (algo == SG_QUERY_BFS) {
+                uint32_t same = 0;
+                for (auto &p : pending)
+                    if (p.q.algo == algo && p.q.graph_id == graph && ++same >= std::max(1u, cfg.msbfs_min)) break;
+                if (same >= std::max(1u, cfg.msbfs_min)) {
+                    one_graph = true;
+                    cap = std::min(cap, 64u);
+                }
+            }
             for (auto it = pending.begin(); it != pending.end() && batch.size() < cap;) {
-                if (it->q.algo == algo) {
+                if (it->q.algo == algo && (!one_graph || it->q.graph_id == graph)) {
                     batch.push_back(*it);
                     it = pending.erase(it);
                 } else {
