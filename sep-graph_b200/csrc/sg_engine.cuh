@@ -169,6 +169,9 @@ struct WarpLB {
     uint32_t beg[32];
     uint32_t src[32];
     TBuffer pay[32];
+    // topology-driven pull: each lane's first and last (possibly shared) segment
+    uint32_t partk[2][32];
+    TBuffer part[2][32];
 };
 
 // A block's own queue of vertices it discovered in a push round and may
@@ -896,42 +899,59 @@ struct EngineKernel {
                 w.beg[lane] = beg;
                 w.pay[lane] = app.PullIdentity();
                 __syncwarp();
-                // four 32-edge batches per step: their index loads, then their
-                // gathers, are issued together (four times the loads in flight
-                // of one batch at a time), then reduced one batch after another
-                constexpr int kUnroll = 4;
-                for (uint32_t eb = 0; eb < total; eb += 32 * kUnroll) {
-                    uint32_t k[kUnroll], src[kUnroll];
-                    TB x[kUnroll];
-#pragma unroll
-                    for (int j = 0; j < kUnroll; ++j) {
-                        const uint32_t e = eb + 32 * j + lane;
-                        k[j] = 0xffffffffu;
-                        src[j] = 0;
-                        if (e < total) {
-                            k[j] = owner(w.excl, e);
-                            src[j] = a.csc.edge_src(w.beg[k[j]] + (e - w.excl[k[j]]));
+                // Each lane reduces one contiguous 1/32 of the warp's concatenated
+                // in-edge lists, four independent gathers at a time, with one owner
+                // search at its start; a destination wholly inside one lane's range
+                // is written by that lane, the (at most two) segments a lane shares
+                // with neighbouring lanes are combined afterwards.
+                const uint32_t per = (total + 31) / 32;
+                const uint32_t lo = min(total, lane * per), hi = min(total, lo + per);
+                w.partk[0][lane] = w.partk[1][lane] = 0xffffffffu;
+                if (lo < hi) {
+                    uint32_t k = owner(w.excl, lo);
+                    uint32_t e = lo;
+                    bool first = true;
+                    while (e < hi) {
+                        const uint32_t seg_lo = w.excl[k];
+                        uint32_t seg_hi = total;  // next lane with a larger start
+                        for (uint32_t j = k + 1; j < 32; ++j)
+                            if (w.excl[j] > seg_lo) {
+                                seg_hi = w.excl[j];
+                                break;
+                            }
+                        const uint32_t end = min(hi, seg_hi);
+                        const uint32_t *src = a.csc.edge_source;
+                        const uint32_t off = w.beg[k] - seg_lo;  // CSC edge of e is off + e (mod 2^32)
+                        TB r = app.PullIdentity();
+                        for (; e + 4 <= end; e += 4) {
+                            const uint32_t s0 = __ldg(src + (off + e)), s1 = __ldg(src + (off + e + 1));
+                            const uint32_t s2 = __ldg(src + (off + e + 2)), s3 = __ldg(src + (off + e + 3));
+                            const TB g0 = dev::ld_l2(srcbuf + s0), g1 = dev::ld_l2(srcbuf + s1);
+                            const TB g2 = dev::ld_l2(srcbuf + s2), g3 = dev::ld_l2(srcbuf + s3);
+                            r = app.PullReduce(r, app.PullReduce(app.PullReduce(g0, g1), app.PullReduce(g2, g3)));
                         }
-                    }
-#pragma unroll
-                    for (int j = 0; j < kUnroll; ++j)
-                        x[j] = k[j] != 0xffffffffu ? dev::ld_l2(srcbuf + src[j]) : app.PullIdentity();
-#pragma unroll
-                    for (int j = 0; j < kUnroll; ++j) {
-                        if (eb + 32 * j >= total) break;  // the same in every lane
-                        // segmented reduction: lanes of one destination are contiguous
-                        TB xj = x[j];
-                        const uint32_t kj = k[j];
-#pragma unroll
-                        for (int d = 1; d < 32; d <<= 1) {
-                            const TB y = __shfl_down_sync(dev::kFullMask, xj, d);
-                            const uint32_t ky = __shfl_down_sync(dev::kFullMask, kj, d);
-                            if (lane + d < 32 && ky == kj) xj = app.PullReduce(xj, y);
+                        for (; e < end; ++e) r = app.PullReduce(r, dev::ld_l2(srcbuf + __ldg(src + (off + e))));
+                        const bool shared = seg_lo < lo || seg_hi > hi;  // other lanes hold part of k
+                        if (!shared) {
+                            w.pay[k] = r;
+                        } else {
+                            const int slot = first ? 0 : 1;
+                            w.partk[slot][lane] = k;
+                            w.part[slot][lane] = r;
                         }
-                        const uint32_t kp = __shfl_up_sync(dev::kFullMask, kj, 1);
-                        if (kj != 0xffffffffu && (lane == 0 || kp != kj)) w.pay[kj] = app.PullReduce(w.pay[kj], xj);
-                        __syncwarp();
+                        first = false;
+                        // next destination with edges
+                        while (k < 31 && w.excl[k + 1] <= e) ++k;
                     }
+                }
+                __syncwarp();
+                {
+                    TB r = w.pay[lane];
+                    for (uint32_t j = 0; j < 32; ++j) {
+                        if (w.partk[0][j] == lane) r = app.PullReduce(r, w.part[0][j]);
+                        if (w.partk[1][j] == lane) r = app.PullReduce(r, w.part[1][j]);
+                    }
+                    w.pay[lane] = r;
                 }
                 __syncwarp();
                 if (v < N && deg > 0) accumulate<App, TB, TW>(app, a.csc_w, v, v, beg, a.buffer + v, w.pay[lane]);
