@@ -89,6 +89,7 @@ struct Counters {
     uint32_t heavy_enq[4];
     unsigned long long scout[4];
     uint32_t middle_count, error;
+    uint32_t active_count;  // active vertices of a round whose worklist nobody reads (forced TD)
     uint32_t heavy_count[2], chunk_count[2];  // heavy-vertex tables, one set per round parity
     unsigned long long edges_processed;
 };
@@ -766,7 +767,7 @@ struct EngineKernel {
     // CombineValueBuffer over every vertex; scheduled vertices form the middle
     // list (variants/common.cuh:17-84).  `sync` writes the combined buffer to
     // tmp (SYNC_PULL_*), else back into buffer (ASYNC_PULL_DD, algo_variants.cuh:842-849).
-    static __device__ void combine_all(App &app, const Args &a, bool sync) {
+    static __device__ void combine_all(App &app, const Args &a, bool sync, bool build_middle = true) {
         const uint32_t lane = dev::lane_id();
         const uint32_t N = a.csr.nnodes;
         Counters *n = &a.ctrl->cnt;
@@ -781,7 +782,7 @@ struct EngineKernel {
                     a.buffer[v] = pr.first;
                 want = pr.second;
             }
-            dev::warp_append(a.middle, &n->middle_count, a.csr.nnodes, want, v, &n->error);
+            if (build_middle) dev::warp_append(a.middle, &n->middle_count, a.csr.nnodes, want, v, &n->error);
         }
     }
 
@@ -991,10 +992,24 @@ struct EngineKernel {
     }
 
     // RebuildWorklist (driver.cuh:162-178): active vertices -> worklist `slot`.
+    // Under a forced topology-driven variant every round scans all vertices and
+    // no round reads the worklist, so only the active vertices are counted (for
+    // termination and the trace), without queued bits or appends.
+    static __device__ __forceinline__ bool count_only(const Args &a) {
+        return a.p.forced == V_SYNC_PULL_TD || a.p.forced == V_ASYNC_PUSH_TD;
+    }
+
     static __device__ void rebuild(App &app, const Args &a, uint32_t slot, Acc &acc) {
         const uint32_t lane = dev::lane_id();
         const uint32_t N = a.csr.nnodes;
         Counters *n = &a.ctrl->cnt;
+        if (count_only(a)) {
+            uint32_t cnt = 0;
+            for (uint32_t v = gthread(); v < N; v += nthreads()) cnt += app.App::IsActiveNode(v, dev::ld_l2(a.buffer + v));
+            cnt = dev::warp_sum(cnt);
+            if (lane == 0 && cnt) atomicAdd(&n->active_count, cnt);
+            return;
+        }
         for (uint32_t base = gwarp() * 32; base < N; base += nwarps() * 32) {
             const uint32_t v = base + lane;
             bool act = false;
@@ -1129,7 +1144,7 @@ struct EngineKernel {
         const float round_ms = (float)(now - ps.t_round_start) * 1e-6f;
         ps.vertices_processed += is_dd(var) ? rs.F : a.csr.nnodes;
         const bool prio_push = a.p.priority && var == V_ASYNC_PUSH_DD;
-        const uint32_t out_hi = qc[rs.qhi];
+        const uint32_t out_hi = count_only(a) ? dev::ld_l2(&n->active_count) : qc[rs.qhi];
         const uint32_t out_lo = prio_push ? qc[rs.qlo] : 0;
         ps.output_active = out_hi + out_lo;
         if (a.p.collect) {
@@ -1205,6 +1220,7 @@ struct EngineKernel {
         rs.heavy_expected = a.p.collect ? he[rs.qin] : (rs.F > 0);
         rs.chunks = pend;
         n->middle_count = 0;
+        n->active_count = 0;
         // the previous round's deferred set ran at the start of this round; this
         // round's set either ran inside the round or is now pending
         n->heavy_count[cur ^ 1u] = 0;
@@ -1329,9 +1345,10 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
                 constexpr bool reduce = has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value;
                 K::clear_dirty(a, s);
                 K::release_input_flags(a, s, convert);
-                K::combine_all(app, a, sync);
+                const bool reduce_td = reduce && !dd && lb_pull != LB_NONE;  // scans every vertex, no middle list
+                K::combine_all(app, a, sync, !reduce_td);
                 if (!grid_sync(c, tmo, nop)) return false;
-                if (reduce && !dd && lb_pull != LB_NONE) {
+                if (reduce_td) {
                     K::pull_reduce_td(app, a, s, my_lb, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                     if (!grid_sync(c, tmo, nop)) return false;
