@@ -677,14 +677,19 @@ sg_status prepare_batch(sg_ctx *ctx, sgb::Workspace &ws, std::vector<engine::Bat
     if (!max_bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_bps, B.kernel, kBlockThreads, 0));
     const int bps = std::max(1, std::min(max_bps, o.blocks_per_sm > 0 ? o.blocks_per_sm : 4));
     const uint32_t total_blocks = (uint32_t)(ctx->prop.multiProcessorCount * bps);
-    // Automatic team size: one block per 2M edges of the largest graph (64
-    // BFS/SSSP queries on RMAT scale 22 ran fastest with 37-74 blocks per team,
-    // 1.8x faster than one grid-wide team), and never fewer blocks than it
-    // takes to keep the whole grid busy when the batch has few queries.
+    // Automatic team size.  Equal teams claim queries largest first, so the
+    // batch lasts at least as long as its largest query on one team: a team
+    // gets 4x its edge-proportional share of the grid, blocks * 4 * ne_max /
+    // sum(ne), and at least one block per 2M edges of the largest graph.
+    // Measured on B200 (592 blocks): 256 SSSP queries over RMAT scales 12-20
+    // ran in 27-30 ms with 24-49 blocks per team against 72 ms with 7; 256 on
+    // RMAT-14 fastest with 8-10; 64 BFS on RMAT-22 flat from 24 to 148.
     uint32_t team_blocks = (uint32_t)o.team_blocks;
     if (o.team_blocks <= 0) {
-        team_blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ne_max >> 21, total_blocks));
-        team_blocks = std::max(team_blocks, total_blocks / n);
+        uint64_t sum_ne = 0;
+        for (auto *g : graphs) sum_ne += g->ne;
+        const uint64_t share = (4ull * total_blocks * ne_max + sum_ne - 1) / std::max<uint64_t>(1, sum_ne);
+        team_blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(std::max(ne_max >> 21, share), total_blocks));
     }
     team_blocks = std::max(1u, std::min(team_blocks, total_blocks));
     const uint32_t n_teams = std::max(1u, std::min(n, total_blocks / team_blocks));
