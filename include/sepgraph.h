@@ -155,6 +155,29 @@ sg_status sg_graph_create_from_host(sg_ctx *ctx, const sg_hgraph *h, uint32_t fl
 sg_status sg_graph_destroy(sg_graph *g);
 sg_status sg_graph_info(const sg_graph *g, uint32_t *nv, uint64_t *ne, uint64_t *device_bytes, int *weighted);
 
+/* Edge list -> device graph, built on the GPU.  Replaces the preprocessing of
+ * the reference's converter (samples/tools/gtools.cpp:56-328) together with the
+ * CSR construction and csr_tocsc (csr_graph.h:329-397) that Engine::LoadGraph
+ * runs on the host.  src/dst/weights hold m entries (host or device memory;
+ * weights may be NULL).  Within a row, edges keep their input order unless a
+ * flag orders them; the CSC view is built on the device as for sg_graph_create.
+ * Failure: SG_ERR_INVALID_ARG for an endpoint >= nv or more than 2^32-2 entries
+ * (after --d2ud doubling). */
+#define SG_BUILD_DESELF_CYCLE 0x1u /* gtools --deself_cycle: drop edges u->u */
+#define SG_BUILD_DEDUPLICATE 0x2u  /* gtools --deduplicate: per source keep the first edge to each destination */
+#define SG_BUILD_D2UD 0x4u         /* gtools --d2ud: add every reverse edge; rows sorted by destination and
+                                      deduplicated, the first inserted edge's weight kept; implies
+                                      SG_GRAPH_SYMMETRIC */
+#define SG_BUILD_SORT_ROWS 0x8u    /* rows ordered by destination (input order among equal destinations) */
+sg_status sg_graph_build(sg_ctx *ctx, uint32_t nv, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                         const uint32_t *weights, uint32_t build_flags, uint32_t graph_flags, sg_graph **out);
+/* Copies a device graph's CSR (csc == 0) or in-edge CSC view (csc != 0) into
+ * caller buffers (host or device): offsets nv+1, indices ne, weights ne (NULL
+ * skips them).  SG_ERR_UNSUPPORTED when the graph has no CSC view.  No
+ * reference counterpart (the reference keeps its CSC on the host,
+ * csr_graph.h:1596-1783). */
+sg_status sg_graph_copy_out(const sg_graph *g, int csc, uint32_t *offsets, uint32_t *indices, uint32_t *weights);
+
 sg_status sg_options_default(sg_options *opt);
 
 /* ------------------------------------------------------------------ algorithms */

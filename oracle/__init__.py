@@ -64,6 +64,7 @@ def ref() -> C.CDLL:
         L.sgref_pagerank_check.argtypes = [C.c_uint32, _P, _P, C.c_int]
         L.sgref_bc.argtypes = [C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P]
         L.sgref_bc_check.argtypes = [C.c_uint32, _P, _P]
+        L.sgref_csr_tocsc.argtypes = [C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, _P]
         _r = L
     return _r
 
@@ -120,6 +121,68 @@ def bc_f64(offsets, indices, src):
     return bc, sg, lv
 
 
+# ---------------------------------------------------------------- graph construction
+def csr_tocsc(offsets, indices, weights=None):
+    """CSR -> CSC as csr_tocsc builds it (include/groute/graphs/csr_graph.h:329-397):
+    a stable counting sort of the edges by destination, so each in-edge list is
+    ordered by source and parallel edges keep their CSR order."""
+    o, i = _u32(offsets), _u32(indices)
+    n = len(o) - 1
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(o.astype(np.int64)))
+    order = np.argsort(i, kind="stable")
+    coff = np.zeros(n + 1, np.uint32)
+    coff[1:] = np.cumsum(np.bincount(i, minlength=n))
+    return coff, src[order], (None if weights is None else _u32(weights)[order])
+
+
+def gtools_build(nv, src, dst, weights=None, deself_cycle=False, deduplicate=False, d2ud=False,
+                 sort_rows=False):
+    """Edge list -> CSR under the reference converter's options
+    (samples/tools/gtools.cpp:56-328), applied to the CSR whose rows hold each
+    source's edges in input order:
+      --deself_cycle (56-128): drop u->u, order kept;
+      --deduplicate (130-197): per source keep the first edge to each
+        destination (with its weight), order kept;
+      --d2ud (199-328): in CSR order every edge (u, v, w) inserts v:w into u's
+        map, then u:w into v's map, first insert wins; rows come out sorted by
+        destination.
+    sort_rows (not a converter option) orders rows by destination, CSR order
+    among equal destinations.  Returns (offsets, indices, weights or None)."""
+    s, d = _u32(src).astype(np.int64), _u32(dst).astype(np.int64)
+    w = None if weights is None else _u32(weights)
+    idx = np.arange(len(s))
+    if deself_cycle:
+        idx = idx[s[idx] != d[idx]]
+    idx = idx[np.argsort(s[idx], kind="stable")]  # CSR order
+    if deduplicate:
+        rank = np.arange(len(idx))
+        order = np.lexsort((rank, d[idx], s[idx]))
+        so, do = s[idx][order], d[idx][order]
+        first = np.ones(len(order), bool)
+        first[1:] = (so[1:] != so[:-1]) | (do[1:] != do[:-1])
+        idx = idx[np.sort(order[first])]
+    rows, cols = s[idx], d[idx]
+    ws = None if w is None else w[idx]
+    if d2ud:
+        r = np.arange(len(idx), dtype=np.int64)
+        R, Cc, T = np.concatenate([rows, cols]), np.concatenate([cols, rows]), np.concatenate([2 * r, 2 * r + 1])
+        order = np.lexsort((T, Cc, R))
+        R, Cc = R[order], Cc[order]
+        first = np.ones(len(order), bool)
+        first[1:] = (R[1:] != R[:-1]) | (Cc[1:] != Cc[:-1])
+        rows, cols = R[first], Cc[first]
+        if ws is not None:
+            ws = np.concatenate([ws, ws])[order][first]
+    elif sort_rows:
+        order = np.lexsort((np.arange(len(rows)), cols, rows))
+        rows, cols = rows[order], cols[order]
+        if ws is not None:
+            ws = ws[order]
+    off = np.zeros(nv + 1, np.uint32)
+    off[1:] = np.cumsum(np.bincount(rows, minlength=nv))
+    return off, cols.astype(np.uint32), (None if ws is None else ws.astype(np.uint32))
+
+
 # ---------------------------------------------------------------- reference (compiled)
 def ref_bfs(offsets, indices, src):
     o, i = _u32(offsets), _u32(indices)
@@ -160,3 +223,36 @@ def ref_bc_check(regression, values) -> int:
     a = np.ascontiguousarray(regression, np.float32)
     b = np.ascontiguousarray(values, np.float32)
     return ref().sgref_bc_check(len(a), _p(a), _p(b))
+
+
+def ref_csr_tocsc(offsets, indices, weights=None):
+    """The reference's own CSCGraph(csr, undirected=false) construction."""
+    o, i = _u32(offsets), _u32(indices)
+    w = None if weights is None else _u32(weights)
+    n, m = len(o) - 1, len(i)
+    co, ci = np.empty(n + 1, np.uint32), np.empty(m, np.uint32)
+    cw = None if w is None else np.empty(m, np.uint32)
+    ref().sgref_csr_tocsc(n, m, _p(o), _p(i), _p(w), _p(co), _p(ci), _p(cw))
+    return co, ci, cw
+
+
+REF_GTOOLS = os.path.join(_HERE, "_ref", "gtools")
+
+
+def ref_gtools_available() -> bool:
+    return os.path.exists(REF_GTOOLS)
+
+
+def ref_gtools(gr_path, out_path, deself_cycle=False, deduplicate=True, d2ud=False):
+    """Runs the reference's converter (samples/tools/gtools.cpp, built by
+    `make -C oracle ref`) on a Galois .gr file; returns its edge list as
+    (src, dst, weights or None) arrays in output order."""
+    b = lambda x: "true" if x else "false"
+    subprocess.run([REF_GTOOLS, f"--graphfile={gr_path}", "--format=gr", f"--output={out_path}",
+                    f"--deself_cycle={b(deself_cycle)}", f"--deduplicate={b(deduplicate)}", f"--d2ud={b(d2ud)}"],
+                   check=True, capture_output=True)
+    rows = np.loadtxt(out_path, dtype=np.int64, ndmin=2) if os.path.getsize(out_path) else np.zeros((0, 2))
+    if rows.size == 0:
+        return np.zeros(0, np.uint32), np.zeros(0, np.uint32), None
+    w = rows[:, 2].astype(np.uint32) if rows.shape[1] > 2 else None
+    return rows[:, 0].astype(np.uint32), rows[:, 1].astype(np.uint32), w

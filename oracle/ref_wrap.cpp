@@ -9,6 +9,7 @@
 //   PageRankCheckErrors        samples/hybrid_pr/hybrid_pr_host.cpp:126-161
 //   BetweennessCentralityHost  samples/hybrid_bc/hybrid_bc_host.cpp:16-92
 //   BCCheckErrors              samples/hybrid_bc/hybrid_bc_host.cpp:94-127
+//   CSCGraph(csr, false)       include/groute/graphs/csr_graph.h:400-441 (csr_tocsc)
 // The graph is bound (not copied) into the reference's host CSRGraph via
 // CSRGraph::Bind (include/groute/graphs/csr_graph.h), exactly as the
 // reference's traversal::Context does for a loaded .gr file.
@@ -110,6 +111,17 @@ int sgref_bc(uint32_t nv, uint32_t ne, const uint32_t *offsets, const uint32_t *
 int sgref_bc_check(uint32_t n, const float *regression, const float *values) {
     std::vector<float> a(regression, regression + n), b(values, values + n);
     return BCCheckErrors(a, b);
+}
+
+int sgref_csr_tocsc(uint32_t nv, uint32_t ne, const uint32_t *offsets, const uint32_t *indices,
+                    const uint32_t *weights, uint32_t *coff, uint32_t *cidx, uint32_t *cw) {
+    groute::graphs::host::CSRGraph g;
+    bind(g, nv, ne, offsets, indices, weights);
+    groute::graphs::host::CSCGraph c(g, false);
+    std::memcpy(coff, c.col_start, sizeof(uint32_t) * (nv + 1));
+    std::memcpy(cidx, c.edge_source, sizeof(uint32_t) * ne);
+    if (weights && cw) std::memcpy(cw, c.edge_weights, sizeof(uint32_t) * ne);
+    return 0;
 }
 
 }  // extern "C"

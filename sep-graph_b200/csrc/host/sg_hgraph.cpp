@@ -449,50 +449,4 @@ sg_status pick_sources(const HostGraph &g, uint32_t n, uint64_t seed, uint32_t *
     return SG_OK;
 }
 
-// Transpose CSR -> CSC (in-edges), sources ascending within each column, as
-// csr_tocsc in include/groute/graphs/csr_graph.h:329-397 produces.
-void transpose(uint32_t nv, uint64_t ne, const uint32_t *off, const uint32_t *idx, const uint32_t *w,
-               std::vector<uint32_t> &coff, std::vector<uint32_t> &cidx, std::vector<uint32_t> &cw) {
-    std::vector<std::atomic<uint32_t>> cnt(nv);
-    for (uint32_t v = 0; v < nv; ++v) cnt[v].store(0, std::memory_order_relaxed);
-    parallel_for(ne, [&](uint64_t b, uint64_t e) {
-        for (uint64_t i = b; i < e; ++i) cnt[idx[i]].fetch_add(1, std::memory_order_relaxed);
-    });
-    coff.assign(nv + 1, 0);
-    for (uint32_t v = 0; v < nv; ++v) coff[v + 1] = coff[v] + cnt[v].load(std::memory_order_relaxed);
-    cidx.resize(ne);
-    if (w) cw.resize(ne);
-    else cw.clear();
-    std::vector<std::atomic<uint32_t>> cur(nv);
-    for (uint32_t v = 0; v < nv; ++v) cur[v].store(coff[v], std::memory_order_relaxed);
-    // Scatter by source ranges; each thread owns a contiguous range of sources,
-    // then every column is sorted by (source, weight) so the result is unique.
-    parallel_for(nv, [&](uint64_t b, uint64_t e) {
-        for (uint64_t u = b; u < e; ++u)
-            for (uint32_t k = off[u]; k < off[u + 1]; ++k) {
-                uint32_t p = cur[idx[k]].fetch_add(1, std::memory_order_relaxed);
-                cidx[p] = (uint32_t)u;
-                if (w) cw[p] = w[k];
-            }
-    });
-    parallel_for_dynamic(nv, 4096, [&](uint64_t b, uint64_t e) {
-        std::vector<std::pair<uint32_t, uint32_t>> tmp;
-        for (uint64_t v = b; v < e; ++v) {
-            uint32_t lo = coff[v], hi = coff[v + 1];
-            if (hi - lo < 2) continue;
-            if (!w) {
-                std::sort(cidx.begin() + lo, cidx.begin() + hi);
-                continue;
-            }
-            tmp.clear();
-            for (uint32_t k = lo; k < hi; ++k) tmp.emplace_back(cidx[k], cw[k]);
-            std::sort(tmp.begin(), tmp.end());
-            for (uint32_t k = lo; k < hi; ++k) {
-                cidx[k] = tmp[k - lo].first;
-                cw[k] = tmp[k - lo].second;
-            }
-        }
-    });
-}
-
 }  // namespace sgb

@@ -30,6 +30,4 @@ sg_status write_gr(const HostGraph &g, const char *path);
 sg_status read_market(const char *path, bool symmetrize, HostGraph &g);
 sg_status max_degree_vertex(const HostGraph &g, uint32_t *vertex, uint32_t *degree);
 sg_status pick_sources(const HostGraph &g, uint32_t n, uint64_t seed, uint32_t *out);
-void transpose(uint32_t nv, uint64_t ne, const uint32_t *off, const uint32_t *idx, const uint32_t *w,
-               std::vector<uint32_t> &coff, std::vector<uint32_t> &cidx, std::vector<uint32_t> &cw);
 }  // namespace sgb

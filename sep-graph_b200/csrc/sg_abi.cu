@@ -19,17 +19,7 @@ using sgb::set_error;
 
 namespace {
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
+using sgb::DeviceGuard;
 
 // Checks an uploaded CSR (offsets start at 0, end at ne and never decrease;
 // every index < nv) and sums the weights, so that a graph whose edges need no
@@ -297,25 +287,28 @@ sg_status sg_options_default(sg_options *opt) {
 
 }  // extern "C"
 
-namespace {
+namespace sgb {
 
-// A graph whose edges need no host-side work (no CSC to build, or a symmetric
-// unweighted one whose CSC aliases the CSR) is uploaded as it is and checked
-// on the device: host or device inputs, one copy each, one validation kernel.
-sg_status create_on_device(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
-                           const uint32_t *weights, uint32_t flags, sg_graph **out) {
+// Every graph is uploaded as it is (host or device inputs, one copy each),
+// checked on the device by one validation kernel, and gets its in-edge (CSC)
+// view from the device transpose: no host loop over the edges.
+sg_status create_graph(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
+                       const uint32_t *weights, uint32_t flags, sg_graph **out) {
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const bool has_csc = !(flags & SG_GRAPH_NO_CSC), symmetric = (flags & SG_GRAPH_SYMMETRIC) != 0;
+    const bool full_csc = has_csc && !symmetric;
     const size_t b_row = al(4ull * (nv + 1)), b_col = al(4ull * std::max<uint64_t>(ne, 1));
     const size_t b_w = weights ? b_col : 0;
-    const size_t total = b_row + b_col + b_w + al(sizeof(CsrCheck));
+    const size_t b_csr = b_row + b_col + b_w;
+    const size_t total = b_csr * (full_csc ? 2 : 1) + al(sizeof(CsrCheck));
     sg_graph *g = new (std::nothrow) sg_graph;
     if (!g) return SG_ERR_OUT_OF_MEMORY;
     g->ctx = ctx;
     g->nv = nv;
     g->ne = ne;
     g->weighted = weights != nullptr;
-    g->symmetric = flags & SG_GRAPH_SYMMETRIC;
-    g->has_csc = !(flags & SG_GRAPH_NO_CSC);
+    g->symmetric = symmetric;
+    g->has_csc = has_csc;
     cudaError_t e = cudaMalloc(&g->arena, total);
     if (e != cudaSuccess) {
         delete g;
@@ -323,20 +316,24 @@ sg_status create_on_device(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t
     }
     g->arena_bytes = total;
     char *p = (char *)g->arena;
-    g->row = (uint32_t *)p;
-    p += b_row;
-    g->col = (uint32_t *)p;
-    p += b_col;
-    if (weights) {
-        g->w = (uint32_t *)p;
-        p += b_w;
-    }
-    CsrCheck *dchk = (CsrCheck *)p;
-    if (g->has_csc) {  // symmetric: CSC aliases CSR (csr_graph.h:405-410)
+    auto carve = [&](size_t bytes) {
+        uint32_t *q = (uint32_t *)p;
+        p += bytes;
+        return q;
+    };
+    g->row = carve(b_row);
+    g->col = carve(b_col);
+    if (weights) g->w = carve(b_w);
+    if (full_csc) {
+        g->crow = carve(b_row);
+        g->ccol = carve(b_col);
+        if (weights) g->cw = carve(b_w);
+    } else if (has_csc) {  // symmetric: CSC aliases CSR (csr_graph.h:405-410)
         g->crow = g->row;
         g->ccol = g->col;
         g->cw = g->w;
     }
+    CsrCheck *dchk = (CsrCheck *)p;
     const cudaStream_t s = ctx->stream;
     CsrCheck hchk{0u, 0xffffffffu, ~0ull, 0.0};
     uint32_t bad_dst = 0;
@@ -366,12 +363,17 @@ sg_status create_on_device(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t
         return fail(set_error(ctx, SG_ERR_INVALID_ARG, "edge %llu points to vertex %u >= nv", hchk.first_bad_edge, bad_dst));
     }
     g->weight_sum = weights ? hchk.weight_sum : (double)ne;
+    sg_status st = SG_OK;
+    if (full_csc) st = device_transpose(ctx, nv, ne, g->row, g->col, g->w, g->crow, g->ccol, g->cw);
+    else if (has_csc && weights) st = symmetric_weighted_csc(ctx, g);
+    if (st == SG_OK) st = sgb::cuda_status(ctx, cudaStreamSynchronize(s), "graph transpose");
+    if (st != SG_OK) return fail(st);
     ctx->live_graphs++;
     *out = g;
     return SG_OK;
 }
 
-}  // namespace
+}  // namespace sgb
 
 extern "C" {
 
@@ -381,123 +383,7 @@ sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t 
     if (ne >= (1ull << 32)) return set_error(ctx, SG_ERR_INVALID_ARG, "edge count %llu exceeds uint32", (unsigned long long)ne);
     *out = nullptr;
     DeviceGuard dg(ctx->device);
-    if ((flags & SG_GRAPH_NO_CSC) || ((flags & SG_GRAPH_SYMMETRIC) && !weights))
-        return create_on_device(ctx, nv, ne, offsets, indices, weights, flags, out);
-    // Inputs may be host or device memory; validation and the CSC build run on host copies.
-    const bool dev_in = sgb::is_device_ptr(offsets, ctx->device);
-    std::vector<uint32_t> h_off, h_idx, h_w;
-    const uint32_t *off = offsets, *idx = indices, *w = weights;
-    if (dev_in) {
-        h_off.resize(nv + 1);
-        h_idx.resize(ne);
-        SG_TRY_CUDA(ctx, cudaMemcpy(h_off.data(), offsets, 4 * (nv + 1), cudaMemcpyDeviceToHost));
-        if (ne) SG_TRY_CUDA(ctx, cudaMemcpy(h_idx.data(), indices, 4 * ne, cudaMemcpyDeviceToHost));
-        if (weights) {
-            h_w.resize(ne);
-            if (ne) SG_TRY_CUDA(ctx, cudaMemcpy(h_w.data(), weights, 4 * ne, cudaMemcpyDeviceToHost));
-        }
-        off = h_off.data();
-        idx = h_idx.data();
-        w = weights ? h_w.data() : nullptr;
-    }
-    if (off[0] != 0 || off[nv] != ne) return set_error(ctx, SG_ERR_INVALID_ARG, "offsets[0] must be 0 and offsets[nv] == ne");
-    for (uint32_t v = 0; v < nv; ++v)
-        if (off[v + 1] < off[v]) return set_error(ctx, SG_ERR_INVALID_ARG, "offsets not monotone at %u", v);
-    for (uint64_t e = 0; e < ne; ++e)
-        if (idx[e] >= nv) return set_error(ctx, SG_ERR_INVALID_ARG, "edge %llu points to vertex %u >= nv", (unsigned long long)e, idx[e]);
-
-    sg_graph *g = new (std::nothrow) sg_graph;
-    if (!g) return SG_ERR_OUT_OF_MEMORY;
-    g->ctx = ctx;
-    g->nv = nv;
-    g->ne = ne;
-    g->weighted = w != nullptr;
-    g->symmetric = flags & SG_GRAPH_SYMMETRIC;
-    g->has_csc = !(flags & SG_GRAPH_NO_CSC);
-    double ws = 0;
-    if (w)
-        for (uint64_t e = 0; e < ne; ++e) ws += w[e];
-    g->weight_sum = w ? ws : (double)ne;
-
-    // A symmetric graph's CSC aliases its CSR (csr_graph.h:405-410).  With edge
-    // weights that alias is only right when w(u->v) == w(v->u) edge by edge, so
-    // a weighted symmetric graph is transposed: an identical structure is still
-    // aliased and only weights that differ get their own CSC weight array; a
-    // structure whose transpose lists neighbours in another order gets a full CSC.
-    std::vector<uint32_t> coff, cidx, cw;
-    bool build_csc = g->has_csc && !g->symmetric;
-    bool own_cw = false;
-    if (build_csc || (g->has_csc && w)) sgb::transpose(nv, ne, off, idx, w, coff, cidx, cw);
-    if (g->has_csc && g->symmetric && w) {
-        const bool same_structure = std::equal(coff.begin(), coff.end(), off) && std::equal(cidx.begin(), cidx.end(), idx);
-        build_csc = !same_structure;
-        own_cw = same_structure && !std::equal(cw.begin(), cw.end(), w);
-    }
-
-    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-    const size_t b_row = al(4ull * (nv + 1)), b_col = al(4ull * std::max<uint64_t>(ne, 1));
-    const size_t b_w = w ? b_col : 0;
-    size_t total = b_row + b_col + b_w;
-    if (build_csc) total += b_row + b_col + b_w;
-    if (own_cw) total += b_w;
-    cudaError_t e = cudaMalloc(&g->arena, total);
-    if (e != cudaSuccess) {
-        delete g;
-        return sgb::cuda_status(ctx, e, "graph arena");
-    }
-    g->arena_bytes = total;
-    char *p = (char *)g->arena;
-    g->row = (uint32_t *)p;
-    p += b_row;
-    g->col = (uint32_t *)p;
-    p += b_col;
-    if (w) {
-        g->w = (uint32_t *)p;
-        p += b_w;
-    }
-    if (build_csc) {
-        g->crow = (uint32_t *)p;
-        p += b_row;
-        g->ccol = (uint32_t *)p;
-        p += b_col;
-        if (w) {
-            g->cw = (uint32_t *)p;
-            p += b_w;
-        }
-    } else if (g->has_csc) {  // symmetric: CSC aliases CSR
-        g->crow = g->row;
-        g->ccol = g->col;
-        g->cw = g->w;
-        if (own_cw) {
-            g->cw = (uint32_t *)p;
-            p += b_w;
-        }
-    }
-    sg_status st = SG_OK;
-    auto cp = [&](void *dst, const void *src, size_t bytes) {
-        if (st == SG_OK && bytes) {
-            cudaError_t ce = cudaMemcpy(dst, src, bytes, cudaMemcpyDefault);
-            if (ce != cudaSuccess) st = sgb::cuda_status(ctx, ce, "graph upload");
-        }
-    };
-    cp(g->row, off, 4ull * (nv + 1));
-    cp(g->col, idx, 4ull * ne);
-    if (w) cp(g->w, w, 4ull * ne);
-    if (build_csc) {
-        cp(g->crow, coff.data(), 4ull * (nv + 1));
-        cp(g->ccol, cidx.data(), 4ull * ne);
-        if (w) cp(g->cw, cw.data(), 4ull * ne);
-    } else if (own_cw) {
-        cp(g->cw, cw.data(), 4ull * ne);
-    }
-    if (st != SG_OK) {
-        cudaFree(g->arena);
-        delete g;
-        return st;
-    }
-    ctx->live_graphs++;
-    *out = g;
-    return SG_OK;
+    return sgb::create_graph(ctx, nv, ne, offsets, indices, weights, flags, out);
 }
 
 sg_status sg_graph_create_from_host(sg_ctx *ctx, const sg_hgraph *h, uint32_t flags, sg_graph **out) {
@@ -557,6 +443,20 @@ sg_status sg_graph_info(const sg_graph *g, uint32_t *nv, uint64_t *ne, uint64_t 
     if (ne) *ne = g->ne;
     if (device_bytes) *device_bytes = g->arena_bytes;
     if (weighted) *weighted = g->weighted;
+    return SG_OK;
+}
+
+sg_status sg_graph_copy_out(const sg_graph *g, int csc, uint32_t *offsets, uint32_t *indices, uint32_t *weights) {
+    if (!g || !g->ctx) return SG_ERR_INVALID_ARG;
+    sg_ctx *ctx = g->ctx;
+    if (csc && !g->has_csc) return set_error(ctx, SG_ERR_UNSUPPORTED, "graph was created without a CSC view");
+    if (weights && !g->weighted) return set_error(ctx, SG_ERR_INVALID_ARG, "graph has no weights");
+    DeviceGuard dg(ctx->device);
+    const uint32_t *row = csc ? g->crow : g->row, *col = csc ? g->ccol : g->col, *w = csc ? g->cw : g->w;
+    SG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (offsets) SG_TRY_CUDA(ctx, cudaMemcpy(offsets, row, 4ull * (g->nv + 1), cudaMemcpyDefault));
+    if (indices && g->ne) SG_TRY_CUDA(ctx, cudaMemcpy(indices, col, 4ull * g->ne, cudaMemcpyDefault));
+    if (weights && g->ne) SG_TRY_CUDA(ctx, cudaMemcpy(weights, w, 4ull * g->ne, cudaMemcpyDefault));
     return SG_OK;
 }
 

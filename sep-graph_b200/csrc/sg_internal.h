@@ -24,4 +24,16 @@ double graph_weight_sum(const sg_graph *g);
 sg_graph *graph_view(sg_graph *g, sg_ctx *ctx);
 void graph_view_destroy(sg_graph *view);
 
+// Device graph from a CSR (host or device arrays): one upload, validation on
+// the device, and the in-edge (CSC) view from the device transpose.
+sg_status create_graph(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
+                       const uint32_t *weights, uint32_t flags, sg_graph **out);
+// CSR -> CSC on the device (all pointers device memory), ordered as csr_tocsc
+// orders it: by source, parallel edges by CSR position.
+sg_status device_transpose(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *row, const uint32_t *col,
+                           const uint32_t *w, uint32_t *crow, uint32_t *ccol, uint32_t *cw);
+// In-edge view of a symmetric weighted graph: the CSR alias where the
+// transpose is identical, else its own weights or a full CSC.
+sg_status symmetric_weighted_csc(sg_ctx *ctx, sg_graph *g);
+
 }  // namespace sgb

@@ -141,6 +141,19 @@ inline sg_status device_error_status(uint32_t bits) {
     return SG_OK;
 }
 
+// Makes `dev` current for the guard's lifetime.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
 // Is `p` device memory of the context's device (output written in place)?
 inline bool is_device_ptr(const void *p, int device) {
     if (!p) return false;

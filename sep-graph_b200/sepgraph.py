@@ -33,6 +33,10 @@ VARIANTS = {
 VARIANT_NAMES = {v: k.upper() for k, v in VARIANTS.items() if v >= 0}
 GRAPH_SYMMETRIC = 0x1
 GRAPH_NO_CSC = 0x2
+BUILD_DESELF_CYCLE = 0x1  # sg_graph_build flags (the reference converter's options)
+BUILD_DEDUPLICATE = 0x2
+BUILD_D2UD = 0x4
+BUILD_SORT_ROWS = 0x8
 GEN_SYMMETRIC = 0x1
 GEN_KEEP_SELF_LOOPS = 0x2
 GEN_KEEP_DUPLICATES = 0x4
@@ -158,6 +162,8 @@ def load() -> C.CDLL:
         "sg_graph_create": (C.c_int, [_P, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_uint32, C.POINTER(_P)]),
         "sg_graph_create_from_host": (C.c_int, [_P, _P, C.c_uint32, C.POINTER(_P)]),
         "sg_graph_destroy": (C.c_int, [_P]),
+        "sg_graph_build": (C.c_int, [_P, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
+        "sg_graph_copy_out": (C.c_int, [_P, C.c_int, _P, _P, _P]),
         "sg_graph_info": (C.c_int, [_P, _U32P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_int)]),
         "sg_options_default": (C.c_int, [C.POINTER(Options)]),
@@ -449,6 +455,25 @@ class Context:
                                       C.byref(g)), "graph_create", self._c)
         return Graph(self, g)
 
+    def build_graph(self, nv: int, src, dst, weights=None, deself_cycle=False, deduplicate=False, d2ud=False,
+                    sort_rows=False, symmetric=False, no_csc=False, m=None) -> "Graph":
+        """Edge list -> device graph built on the GPU (sg_graph_build); the flags are the
+        reference converter's --deself_cycle / --deduplicate / --d2ud plus row ordering.
+        Arrays may be numpy (converted to uint32), torch tensors, or int device pointers
+        (then pass m)."""
+        def u32(a):
+            return np.ascontiguousarray(a, dtype=np.uint32) if isinstance(a, (np.ndarray, list, tuple)) else a
+        src, dst, weights = u32(src), u32(dst), u32(weights)
+        if m is None:
+            m = len(src)
+        bflags = ((BUILD_DESELF_CYCLE if deself_cycle else 0) | (BUILD_DEDUPLICATE if deduplicate else 0)
+                  | (BUILD_D2UD if d2ud else 0) | (BUILD_SORT_ROWS if sort_rows else 0))
+        gflags = (GRAPH_SYMMETRIC if symmetric else 0) | (GRAPH_NO_CSC if no_csc else 0)
+        g = _P()
+        _check(load().sg_graph_build(self._c, nv, m, _ptr(src), _ptr(dst), _ptr(weights), bflags, gflags,
+                                     C.byref(g)), "sg_graph_build", self._c)
+        return Graph(self, g)
+
     def close(self):
         """Releases the context; graphs still open on it are released first."""
         if self._c:
@@ -583,6 +608,16 @@ class Graph:
     @property
     def nv(self) -> int:
         return self.info()["nv"]
+
+    def copy_out(self, csc: bool = False):
+        """(offsets, indices, weights or None) of the CSR, or of the in-edge CSC view."""
+        inf = self.info()
+        off = np.empty(inf["nv"] + 1, np.uint32)
+        idx = np.empty(inf["ne"], np.uint32)
+        w = np.empty(inf["ne"], np.uint32) if inf["weighted"] else None
+        _check(load().sg_graph_copy_out(self._g, 1 if csc else 0, _ptr(off), _ptr(idx), _ptr(w)),
+               "sg_graph_copy_out", self.ctx.handle)
+        return off, idx, w
 
     def _stats(self, trace_capacity: int):
         st = Stats()

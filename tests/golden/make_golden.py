@@ -1,14 +1,20 @@
 """Regenerates tests/golden/*.npz: small graphs and the outputs of the
 reference's own host checkers (BFSHost, SSSPHostNaive, PageRankHost,
 BetweennessCentralityHost) compiled from the reference sources into
-oracle/_ref/libsgref.so (`make -C oracle ref`).
+oracle/_ref/libsgref.so (`make -C oracle ref`); and tests/golden/convert/*.npz:
+edge lists with the output of the reference's graph converter
+(samples/tools/gtools.cpp, built as oracle/_ref/gtools) under every
+combination of --deself_cycle/--deduplicate/--d2ud, and the reference's
+CSCGraph transpose (csr_tocsc) of the edge list's CSR.
 
 Run from the repository root:  python tests/golden/make_golden.py
 The fixtures pin the oracle restatement (oracle/sg_oracle.c) on machines
 where the reference tree is not available.
 """
 import os
+import shutil
 import sys
+import tempfile
 
 import numpy as np
 
@@ -54,7 +60,60 @@ def cases():
     yield "loops_dups5", off, idx, np.array([2, 7, 1, 3, 5, 1, 4, 2, 6], np.uint32), 0
 
 
+def build_cases():
+    rng = np.random.default_rng(11)
+    for name, nv, m, weighted in (("mixed40w", 40, 300, True), ("mixed25", 25, 120, False),
+                                  ("hub300w", 300, 2500, True)):
+        s = rng.integers(0, nv, m).astype(np.uint32)
+        d = rng.integers(0, nv, m).astype(np.uint32)
+        if name.startswith("hub"):  # one source and one destination with many parallel edges
+            s[: m // 3] = 7
+            d[m // 3: 2 * m // 3] = 7
+        w = rng.integers(1, 9, m).astype(np.uint32) if weighted else None
+        yield name, nv, s, d, w
+    # the first inserted edge wins under --d2ud: (1,5) comes first in CSR order
+    yield "d2ud_order6", 6, np.array([5, 1, 2, 2], np.uint32), np.array([1, 5, 2, 3], np.uint32), \
+        np.array([10, 20, 30, 40], np.uint32)
+    yield "loops4", 4, np.array([0, 1, 1, 3, 3], np.uint32), np.array([0, 1, 1, 3, 2], np.uint32), None
+    yield "empty3", 3, np.zeros(0, np.uint32), np.zeros(0, np.uint32), None
+
+
+def stable_csr(nv, s, d, w):
+    o = np.argsort(s, kind="stable")
+    off = np.zeros(nv + 1, np.uint32)
+    off[1:] = np.cumsum(np.bincount(s, minlength=nv))
+    return off, d[o].astype(np.uint32), (None if w is None else w[o].astype(np.uint32))
+
+
+def main_build():
+    if not oracle.ref_gtools_available():
+        sys.exit("oracle/_ref/gtools missing: run make -C oracle ref")
+    os.makedirs(os.path.join(OUT, "convert"), exist_ok=True)
+    tmp = tempfile.mkdtemp(dir=OUT)
+    for name, nv, s, d, w in build_cases():
+        rec = dict(nv=np.uint32(nv), src=s, dst=d)
+        if w is not None:
+            rec["weights"] = w
+        off, idx, ww = stable_csr(nv, s, d, w)
+        co, ci, cw = oracle.ref_csr_tocsc(off, idx, ww)
+        rec["csc_offsets"], rec["csc_indices"] = co, ci
+        if cw is not None:
+            rec["csc_weights"] = cw
+        gr = os.path.join(tmp, "g.gr")
+        sg.HostGraph.from_csr(off, idx, ww).write_gr(gr)
+        for code in range(8):
+            ds, dd, du = bool(code & 1), bool(code & 2), bool(code & 4)
+            rs, rd, rw = oracle.ref_gtools(gr, os.path.join(tmp, "o.txt"), ds, dd, du)
+            rec[f"g{code}_src"], rec[f"g{code}_dst"] = rs, rd
+            if rw is not None:
+                rec[f"g{code}_w"] = rw
+        np.savez_compressed(os.path.join(OUT, "convert", f"{name}.npz"), **rec)
+        print("convert", name, nv, len(s))
+    shutil.rmtree(tmp)
+
+
 def main():
+    main_build()
     if not oracle.ref_available():
         sys.exit("oracle/_ref/libsgref.so missing: run make -C oracle ref")
     for name, off, idx, w, src in cases():

@@ -72,3 +72,74 @@ def test_oracle_plants_detected():
     if oracle.ref_available():
         r = oracle.ref().sgref_bfs_check(len(lv), bad.ctypes.data, g["bfs"].ctypes.data)
         assert r == 1
+
+
+# ---------------------------------------------------------------- graph construction
+CONVERT = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "convert", "*.npz")))
+
+
+def _rows_of(off):
+    return np.repeat(np.arange(len(off) - 1, dtype=np.uint32), np.diff(off.astype(np.int64)))
+
+
+def _stable_csr(nv, s, d, w):
+    o = np.argsort(s, kind="stable")
+    off = np.zeros(nv + 1, np.uint32)
+    off[1:] = np.cumsum(np.bincount(s, minlength=nv))
+    return off, d[o].astype(np.uint32), (None if w is None else w[o].astype(np.uint32))
+
+
+@pytest.mark.parametrize("path", CONVERT, ids=[os.path.basename(p)[:-4] for p in CONVERT])
+def test_converter_oracle_matches_golden(path):
+    """oracle.gtools_build against the reference converter's own output, all eight
+    --deself_cycle/--deduplicate/--d2ud combinations; oracle.csr_tocsc against the
+    reference's CSCGraph."""
+    g = _load(path)
+    nv, w = int(g["nv"]), g.get("weights")
+    for code in range(8):
+        off, idx, ww = oracle.gtools_build(nv, g["src"], g["dst"], w, code & 1, code & 2, code & 4)
+        assert np.array_equal(_rows_of(off), g[f"g{code}_src"]), code
+        assert np.array_equal(idx, g[f"g{code}_dst"]), code
+        if w is not None:
+            assert np.array_equal(ww, g[f"g{code}_w"]), code
+    co, ci, cw = oracle.csr_tocsc(*_stable_csr(nv, g["src"], g["dst"], w))
+    assert np.array_equal(co, g["csc_offsets"]) and np.array_equal(ci, g["csc_indices"])
+    if w is not None:
+        assert np.array_equal(cw, g["csc_weights"])
+
+
+def test_converter_golden_covers_first_insert_rule():
+    """d2ud_order6: edge 5->1 (w 10) comes before 1->5 (w 20) in the input, but 1->5
+    is first in CSR order, so both directions keep weight 20."""
+    g = _load(os.path.join(os.path.dirname(__file__), "golden", "convert", "d2ud_order6.npz"))
+    src, dst, w = g["g4_src"], g["g4_dst"], g["g4_w"]
+    pairs = {(int(a), int(b)): int(c) for a, b, c in zip(src, dst, w)}
+    assert pairs[(1, 5)] == 20 and pairs[(5, 1)] == 20
+
+
+@pytest.mark.skipif(not oracle.ref_gtools_available(), reason="reference converter not compiled here")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_converter_oracle_vs_reference_random(seed, tmp_path):
+    rng = np.random.default_rng(seed)
+    for trial in range(6):
+        nv, m = int(rng.integers(1, 50)), int(rng.integers(0, 400))
+        s = rng.integers(0, nv, m).astype(np.uint32)
+        d = rng.integers(0, nv, m).astype(np.uint32)
+        w = rng.integers(1, 9, m).astype(np.uint32) if trial % 2 else None
+        off, idx, ww = _stable_csr(nv, s, d, w)
+        gr = str(tmp_path / "g.gr")
+        sg.HostGraph.from_csr(off, idx, ww).write_gr(gr)
+        for code in range(8):
+            rs, rd, rw = oracle.ref_gtools(gr, str(tmp_path / "o.txt"), code & 1, code & 2, code & 4)
+            o2, i2, w2 = oracle.gtools_build(nv, s, d, w, code & 1, code & 2, code & 4)
+            assert np.array_equal(rs, _rows_of(o2)) and np.array_equal(rd, i2), (trial, code)
+            if w is not None:
+                assert np.array_equal(rw, w2), (trial, code)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference checkers not compiled here")
+def test_csr_tocsc_oracle_vs_reference():
+    h = sg.HostGraph.rmat(10, 8, seed=5, keep_self_loops=True, keep_duplicates=True).gen_weights(1, 9, 3)
+    a = oracle.csr_tocsc(h.offsets, h.indices, h.weights)
+    b = oracle.ref_csr_tocsc(h.offsets, h.indices, h.weights)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
