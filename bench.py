@@ -63,7 +63,7 @@ def args_parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--quick", action="store_true", help="headline line only")
     p.add_argument("--served-queries", type=int, default=1000)
-    p.add_argument("--extras", default="per_algo,batched,served", help="extra sections at N=1 (comma list)")
+    p.add_argument("--extras", default="per_algo,batched,served,ingest", help="extra sections at N=1 (comma list)")
     p.add_argument("--scale", type=int, default=SCALE)
     p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc"],
                    help="run one warm-up and one measured solve of that kernel only (for ncu captures)")
@@ -109,7 +109,9 @@ def peak_hbm():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during the timed region: the sampler is started first and the
+    timed region begins only after its first sample arrived (nvidia-smi can take a second
+    to start on a fresh box), so short timed regions still get samples."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -118,25 +120,41 @@ class Clocks:
     def __init__(self, device: int):
         self.device = device
         self.p = None
+        self.lines = []
+        self.t = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line)
 
     def __enter__(self):
+        import threading
+
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 10 and self.p.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()  # keep samples from the timed region on
         except Exception:
             self.p = None
         return self
 
     def __exit__(self, *a):
-        self.out = ""
         if self.p:
-            time.sleep(0.25)
+            time.sleep(0.12)
             self.p.terminate()
             try:
-                self.out, _ = self.p.communicate(timeout=5)
+                self.p.wait(timeout=5)
             except Exception:
                 self.p.kill()
+            if self.t:
+                self.t.join(timeout=5)
+        self.out = "".join(self.lines)
 
     def summary(self):
         rows = [r.split(", ") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
@@ -381,7 +399,7 @@ def run_ours(a):
         extra = {}
         cache = {"rmat22": (h, G)}
         wanted = set(a.extras.split(","))
-        for name, fn in (("per_algo", per_algo), ("batched", batched), ("served", served)):
+        for name, fn in (("per_algo", per_algo), ("batched", batched), ("served", served), ("ingest", ingest)):
             if name not in wanted:
                 continue
             t0 = time.perf_counter()
@@ -616,6 +634,84 @@ def batched(ctx, cache, a):
                                 "plan_same_results": same_p}
     for _, gg in graphs:
         gg.close()
+    return res
+
+
+def _wall_ms(fn, reps=4):
+    """Median wall ms of fn() between device synchronisations (the first call dropped);
+    for host-orchestrated multi-kernel work such as graph construction."""
+    import torch
+
+    ts = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        ts.append((time.perf_counter() - t0) * 1e3)
+        if hasattr(r, "close"):
+            r.close()
+    return statistics.median(ts[1:])
+
+
+def ingest(ctx, cache, a):
+    """Graph construction on the device.  (1) sg_graph_create of a directed weighted
+    RMAT-23 CSR already in HBM: validation plus the csr_tocsc transpose; algorithmic
+    bytes = read CSR + write CSC = 2 * (4(V+1) + 8E).  (2) sg_graph_build of the RMAT-22
+    raw edge stream (self-loops and duplicates kept, shuffled) under the converter's
+    options.  CPU baseline: the reference's CSCGraph construction (csr_tocsc) on the
+    RMAT-21 CSR, one thread; results checked against the oracle on smaller cases by the
+    tests, and here against the host generator's CSR."""
+    import oracle
+    import sepgraph as sg
+    import torch
+
+    peak = peak_hbm()[0]
+    res = {}
+    h = sg.HostGraph.rmat(23, 16, seed=1).gen_weights(1, 64, 2)
+    nv, ne = h.nv, len(h.indices)
+    dev = [torch.from_numpy(x.view(np.int32)).cuda() for x in (h.offsets, h.indices, h.weights)]
+    t_nocsc = _wall_ms(lambda: ctx.graph_from_csr(*dev, nv=nv, ne=ne, no_csc=True))
+    t_csc = _wall_ms(lambda: ctx.graph_from_csr(*dev, nv=nv, ne=ne))
+    t_tr = t_csc - t_nocsc
+    tr_bytes = 2 * (4 * (nv + 1) + 8 * ne)
+    res["transpose_rmat23_dir_w"] = dict(nv=nv, ne=ne, create_no_csc_ms=t_nocsc, create_with_csc_ms=t_csc,
+                                         transpose_ms=t_tr, transpose_Gedges_s=ne / t_tr / 1e6,
+                                         **_roof(tr_bytes, t_tr, peak))
+    del dev, h
+    hc = sg.HostGraph.rmat(21, 16, seed=1).gen_weights(1, 64, 2)
+    if oracle.ref_available():
+        cpu_s = _cpu_time(lambda: oracle.ref_csr_tocsc(hc.offsets, hc.indices, hc.weights), 20.0)
+        kind = "reference CSCGraph (csr_tocsc) compiled from its sources, 1 thread"
+    else:
+        cpu_s = _cpu_time(lambda: oracle.csr_tocsc(hc.offsets, hc.indices, hc.weights), 20.0)
+        kind = "oracle numpy port"
+    res["transpose_rmat23_dir_w"].update(cpu_Gedges_s=len(hc.indices) / cpu_s / 1e9, cpu_sample="RMAT-21 directed weighted",
+                                         cpu_ms=cpu_s * 1e3, cpu=kind)
+    del hc
+
+    raw = sg.HostGraph.rmat(22, 16, seed=1, keep_self_loops=True, keep_duplicates=True)
+    s = np.repeat(np.arange(raw.nv, dtype=np.uint32), np.diff(raw.offsets.astype(np.int64)))
+    d = raw.indices.copy()
+    nv = raw.nv
+    del raw
+    p = np.random.default_rng(9).permutation(len(s))
+    s, d = s[p], d[p]
+    m = len(s)
+    sd, dd = torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda()
+    del s, d, p
+    out = {"edges_in": m}
+    for name, kw in (("csr_input_order", dict(no_csc=True)), ("csr_sorted_rows", dict(sort_rows=True, no_csc=True)),
+                     ("deself_dedup_sorted", dict(deself_cycle=True, deduplicate=True, sort_rows=True, no_csc=True)),
+                     ("deself_d2ud", dict(deself_cycle=True, d2ud=True))):
+        t = _wall_ms(lambda: ctx.build_graph(nv, sd, dd, m=m, **kw))
+        out[name] = {"ms": t, "Medges_in_s": m / t / 1e3}
+    G = ctx.build_graph(nv, sd, dd, m=m, deself_cycle=True, d2ud=True)
+    off, idx, _ = G.copy_out()
+    G.close()
+    hs = sg.HostGraph.rmat(22, 16, symmetric=True, seed=1)
+    out["d2ud_equals_host_symmetric_generator"] = bool(np.array_equal(off, hs.offsets) and np.array_equal(idx, hs.indices))
+    res["build_rmat22_raw_shuffled"] = out
     return res
 
 

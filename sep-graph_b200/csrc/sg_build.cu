@@ -31,6 +31,7 @@ namespace gbuild {
 
 using sepgraph::dev::kFullMask;
 
+constexpr uint32_t kWarpKeys = 256;    // rows up to this many keys sort in one warp's registers
 constexpr uint32_t kSmemKeys = 4096;   // rows up to this many keys sort in shared memory
 constexpr uint32_t kSortThreads = 256;
 constexpr uint32_t kMergeItems = kSmemKeys / kSortThreads;  // outputs per thread in a merge pass
@@ -183,11 +184,76 @@ __device__ __forceinline__ K warp_bitonic(K x, uint32_t lane) {
     return x;
 }
 
-// One warp per 32 rows: rows of 2-32 keys are sorted in place; longer rows are
-// listed (begin, length) for the shared-memory sort or the chunked merge sort.
+// Bitonic sort of 32*E keys held striped across a warp (element r*32+lane in
+// register r): exchanges at distance >= 32 swap registers within a lane,
+// shorter ones go through shuffles.
+template <class K, int E>
+__device__ __forceinline__ void warp_bitonic_regs(K (&x)[E], uint32_t lane) {
+#pragma unroll
+    for (uint32_t k = 2; k <= 32u * E; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const uint32_t jr = j >> 5;
+#pragma unroll
+                for (uint32_t r = 0; r < (uint32_t)E; ++r) {
+                    if ((r & jr) == 0) {
+                        const uint32_t r2 = r | jr;
+                        const bool asc = ((r * 32 + lane) & k) == 0;
+                        const K a = x[r], b = x[r2];
+                        const bool swap = (a > b) == asc;
+                        x[r] = swap ? b : a;
+                        x[r2] = swap ? a : b;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (uint32_t r = 0; r < (uint32_t)E; ++r) {
+                    const K y = __shfl_xor_sync(kFullMask, x[r], j);
+                    const bool asc = ((r * 32 + lane) & k) == 0, lower = (lane & j) == 0;
+                    x[r] = (lower == asc) ? (x[r] < y ? x[r] : y) : (x[r] < y ? y : x[r]);
+                }
+            }
+        }
+    }
+}
+
+template <class K, int E>
+__device__ __forceinline__ void warp_sort_row(K *keys, uint32_t b, uint32_t len, uint32_t lane) {
+    K x[E];
+#pragma unroll
+    for (uint32_t r = 0; r < (uint32_t)E; ++r) {
+        const uint32_t i = r * 32 + lane;
+        x[r] = i < len ? keys[b + i] : key_max<K>();
+    }
+    warp_bitonic_regs<K, E>(x, lane);
+#pragma unroll
+    for (uint32_t r = 0; r < (uint32_t)E; ++r) {
+        const uint32_t i = r * 32 + lane;
+        if (i < len) keys[b + i] = x[r];
+    }
+}
+
+// One warp per listed row of 33-256 keys.
 template <class K>
-__global__ void sort_rows_small_kernel(const uint32_t *off, uint32_t nv, K *keys, uint2 *mid, uint32_t mid_cap,
-                                       uint2 *big, uint32_t big_cap, uint32_t *counts) {
+__global__ void sort_rows_warp_kernel(const uint2 *segs, const uint32_t *count_dev, uint32_t cap, K *keys) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = min(*count_dev, cap);
+    for (uint32_t i = gw; i < n; i += nw) {
+        const uint2 sg = segs[i];
+        if (sg.y <= 64) warp_sort_row<K, 2>(keys, sg.x, sg.y, lane);
+        else if (sg.y <= 128) warp_sort_row<K, 4>(keys, sg.x, sg.y, lane);
+        else warp_sort_row<K, 8>(keys, sg.x, sg.y, lane);
+    }
+}
+
+// One warp per 32 rows: rows of 2-32 keys are sorted in place; longer rows are
+// listed (begin, length) for the one-warp sort (up to kWarpKeys), the
+// shared-memory sort (up to kSmemKeys) or the chunked merge sort.
+template <class K>
+__global__ void sort_rows_small_kernel(const uint32_t *off, uint32_t nv, K *keys, uint2 *wrows, uint32_t wrows_cap,
+                                       uint2 *mid, uint32_t mid_cap, uint2 *big, uint32_t big_cap, uint32_t *counts) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -199,7 +265,10 @@ __global__ void sort_rows_small_kernel(const uint32_t *off, uint32_t nv, K *keys
             len = off[v + 1] - b;
         }
         if (len > 32) {
-            if (len <= kSmemKeys) {
+            if (len <= kWarpKeys) {
+                const uint32_t p = atomicAdd(counts + 2, 1u);
+                if (p < wrows_cap) wrows[p] = make_uint2(b, len);
+            } else if (len <= kSmemKeys) {
                 const uint32_t p = atomicAdd(counts, 1u);
                 if (p < mid_cap) mid[p] = make_uint2(b, len);
             } else {
@@ -302,17 +371,21 @@ sg_status sort_rows(sg_ctx *ctx, const uint32_t *off, uint32_t nv, uint64_t n, K
     if (n < 2) return SG_OK;
     const cudaStream_t s = ctx->stream;
     Tmp tmp(ctx);
-    const uint32_t mid_cap = (uint32_t)(n / 33 + 1), big_cap = (uint32_t)(n / (kSmemKeys + 1) + 1);
-    uint2 *mid, *big;
-    uint32_t *counts;
+    const uint32_t wrows_cap = (uint32_t)(n / 33 + 1), mid_cap = (uint32_t)(n / (kWarpKeys + 1) + 1);
+    const uint32_t big_cap = (uint32_t)(n / (kSmemKeys + 1) + 1);
+    uint2 *wrows, *mid, *big;
+    uint32_t *counts;  // [mid, big, warp rows]
+    SG_TRY_CUDA(ctx, tmp.alloc(&wrows, wrows_cap));
     SG_TRY_CUDA(ctx, tmp.alloc(&mid, mid_cap));
     SG_TRY_CUDA(ctx, tmp.alloc(&big, big_cap));
-    SG_TRY_CUDA(ctx, tmp.alloc(&counts, 2));
-    SG_TRY_CUDA(ctx, cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), s));
-    sort_rows_small_kernel<K><<<grid_for((uint64_t)nv, 256), 256, 0, s>>>(off, nv, keys, mid, mid_cap, big, big_cap, counts);
+    SG_TRY_CUDA(ctx, tmp.alloc(&counts, 3));
+    SG_TRY_CUDA(ctx, cudaMemsetAsync(counts, 0, 3 * sizeof(uint32_t), s));
+    sort_rows_small_kernel<K><<<grid_for((uint64_t)nv, 256), 256, 0, s>>>(off, nv, keys, wrows, wrows_cap, mid, mid_cap,
+                                                                        big, big_cap, counts);
+    sort_rows_warp_kernel<K><<<148 * 8, 256, 0, s>>>(wrows, counts + 2, wrows_cap, keys);
     sort_segments_kernel<K><<<148 * 8, kSortThreads, 0, s>>>(mid, counts, mid_cap, keys);
     SG_TRY_CUDA(ctx, cudaGetLastError());
-    uint32_t hc[2];
+    uint32_t hc[3];
     SG_TRY_CUDA(ctx, cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, s));
     SG_TRY_CUDA(ctx, cudaStreamSynchronize(s));
     const uint32_t nbig = std::min(hc[1], big_cap);
@@ -439,32 +512,54 @@ __global__ void scatter_entries_kernel(EdgeList el, uint32_t *cur, K *keys) {
     }
 }
 
-// Rows sorted by (destination, position): the first key of each destination
-// run survives (samples/tools/gtools.cpp:147-175 and the first-insert-wins map
-// of 211-238).  Count pass (tags == nullptr) writes per-row survivor counts;
-// the second pass writes the survivors' positions at noff[v].
-__global__ void unique_rows_kernel(const uint32_t *off, uint32_t nv, const unsigned long long *keys,
-                                   const uint32_t *noff, uint32_t *ndeg, uint32_t *tags) {
+// Deduplication over rows sorted by (destination, position): entry i survives
+// when it opens its row or its destination differs from entry i-1's, i.e. the
+// first key of each destination run (samples/tools/gtools.cpp:147-175 and the
+// first-insert-wins map of 211-238).  Flat passes: a bitmap of row starts, a
+// ballot word of survivors per 32 entries, a scan of the words' counts, then
+// a coalesced compaction and the new row offsets.
+__global__ void row_starts_kernel(const uint32_t *off, uint32_t nv, uint32_t *starts) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = off[v];
+        if (off[v + 1] > b) atomicOr(starts + (b >> 5), 1u << (b & 31));
+    }
+}
+
+__global__ void unique_flags_kernel(const unsigned long long *keys, uint64_t n, const uint32_t *starts,
+                                    uint32_t *words, uint32_t *counts) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t v = gw; v < nv; v += nw) {
-        const uint32_t b = off[v], e = off[v + 1];
-        uint32_t cnt = 0;
-        const uint32_t out = tags ? noff[v] : 0;
-        for (uint32_t c = b; c < e; c += 32) {
-            const uint32_t i = c + lane;
-            bool first = false;
-            unsigned long long k = 0;
-            if (i < e) {
-                k = keys[i];
-                first = i == b || (keys[i - 1] >> 32) != (k >> 32);
-            }
-            const uint32_t m = __ballot_sync(kFullMask, first);
-            if (tags && first) tags[out + cnt + __popc(m & ((1u << lane) - 1))] = (uint32_t)k;
-            cnt += __popc(m);
+    for (uint64_t w = gw; w * 32 < n; w += nw) {
+        const uint64_t i = w * 32 + lane;
+        bool first = false;
+        if (i < n) {
+            first = ((starts[w] >> lane) & 1u) != 0;  // always set for entry 0
+            if (!first) first = (keys[i] >> 32) != (keys[i - 1] >> 32);
         }
-        if (!tags && lane == 0) ndeg[v] = cnt;
+        const uint32_t word = __ballot_sync(kFullMask, first);
+        if (lane == 0) {
+            words[w] = word;
+            counts[w] = __popc(word);
+        }
+    }
+}
+
+__global__ void unique_compact_kernel(const unsigned long long *keys, uint64_t n, const uint32_t *words,
+                                      const uint32_t *wpos, uint32_t *kept) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t word = words[i >> 5], bit = (uint32_t)i & 31;
+        if ((word >> bit) & 1u) kept[wpos[i >> 5] + __popc(word & ((1u << bit) - 1))] = (uint32_t)keys[i];
+    }
+}
+
+// noff[v] = survivors before entry off[v]; words/wpos have one zero word past
+// the data, so off[nv] == n reads the total.
+__global__ void unique_offsets_kernel(const uint32_t *off, uint32_t nv, const uint32_t *words, const uint32_t *wpos,
+                                      uint32_t *noff) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v <= nv; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = off[v], w = p >> 5;
+        noff[v] = wpos[w] + __popc(words[w] & ((1u << (p & 31)) - 1));
     }
 }
 
@@ -536,15 +631,24 @@ sg_status build_rows(sg_ctx *ctx, Tmp &tmp, const EdgeList &el, bool sorted, boo
         SG_TRY_CUDA(ctx, cudaGetLastError());
         if ((st = sort_rows<unsigned long long>(ctx, off, nv, n, keys)) != SG_OK) return st;
         if (dedup) {
-            uint32_t *ndeg, *noff, *kept;
-            SG_TRY_CUDA(ctx, tmp.alloc(&ndeg, (uint64_t)nv + 1));
+            const uint64_t nwords = (n + 31) / 32 + 1;  // one zero word past the data
+            uint32_t *starts, *words, *wcount, *wpos, *noff, *kept;
+            SG_TRY_CUDA(ctx, tmp.alloc(&starts, nwords));
+            SG_TRY_CUDA(ctx, tmp.alloc(&words, nwords));
+            SG_TRY_CUDA(ctx, tmp.alloc(&wcount, nwords));
+            SG_TRY_CUDA(ctx, tmp.alloc(&wpos, nwords + 1));
             SG_TRY_CUDA(ctx, tmp.alloc(&noff, (uint64_t)nv + 1));
-            unique_rows_kernel<<<grid_for((uint64_t)nv * 32, 256), 256, 0, s>>>(off, nv, keys, nullptr, ndeg, nullptr);
+            SG_TRY_CUDA(ctx, cudaMemsetAsync(starts, 0, 4 * nwords, s));
+            SG_TRY_CUDA(ctx, cudaMemsetAsync(words, 0, 4 * nwords, s));
+            SG_TRY_CUDA(ctx, cudaMemsetAsync(wcount, 0, 4 * nwords, s));
+            row_starts_kernel<<<grid_for(nv, 256), 256, 0, s>>>(off, nv, starts);
+            if (n) unique_flags_kernel<<<grid_for(n, 256), 256, 0, s>>>(keys, n, starts, words, wcount);
             SG_TRY_CUDA(ctx, cudaGetLastError());
             unsigned long long nk = 0;
-            if ((st = exclusive_scan(ctx, tmp, ndeg, nv, noff, &nk)) != SG_OK) return st;
+            if ((st = exclusive_scan(ctx, tmp, wcount, nwords, wpos, &nk)) != SG_OK) return st;
             SG_TRY_CUDA(ctx, tmp.alloc(&kept, nk));
-            unique_rows_kernel<<<grid_for((uint64_t)nv * 32, 256), 256, 0, s>>>(off, nv, keys, noff, nullptr, kept);
+            if (n) unique_compact_kernel<<<grid_for(n, 256), 256, 0, s>>>(keys, n, words, wpos, kept);
+            unique_offsets_kernel<<<grid_for((uint64_t)nv + 1, 256), 256, 0, s>>>(off, nv, words, wpos, noff);
             SG_TRY_CUDA(ctx, cudaGetLastError());
             // without row ordering the survivors go back to input order
             if (!sorted && (st = sort_rows<uint32_t>(ctx, noff, nv, nk, kept)) != SG_OK) return st;
