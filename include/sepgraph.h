@@ -362,6 +362,11 @@ sg_status sg_hgraph_gen_weights(sg_hgraph *h, uint32_t lo, uint32_t hi, uint64_t
 sg_status sg_hgraph_read_gr(const char *path, sg_hgraph **out);
 sg_status sg_hgraph_write_gr(const sg_hgraph *h, const char *path);
 sg_status sg_hgraph_read_market(const char *path, int symmetrize, sg_hgraph **out);
+/* METIS graph file (ReadGraph, src/utils/parser.cpp:230-396): 1-based
+ * adjacency lists in file order, every undirected edge listed twice; edge
+ * weights when fmt's last digit is 1; vertex sizes/weights are skipped.
+ * SG_ERR_FORMAT when the entry count differs from twice the header's m. */
+sg_status sg_hgraph_read_metis(const char *path, sg_hgraph **out);
 /* Pointers stay valid until sg_hgraph_destroy. weights is NULL when unweighted. */
 sg_status sg_hgraph_info(const sg_hgraph *h, uint32_t *nv, uint64_t *ne, const uint32_t **offsets,
                          const uint32_t **indices, const uint32_t **weights);

@@ -243,12 +243,13 @@ def ref_gtools_available() -> bool:
     return os.path.exists(REF_GTOOLS)
 
 
-def ref_gtools(gr_path, out_path, deself_cycle=False, deduplicate=True, d2ud=False):
+def ref_gtools(gr_path, out_path, deself_cycle=False, deduplicate=True, d2ud=False, fmt="gr"):
     """Runs the reference's converter (samples/tools/gtools.cpp, built by
-    `make -C oracle ref`) on a Galois .gr file; returns its edge list as
-    (src, dst, weights or None) arrays in output order."""
+    `make -C oracle ref`) on a graph file (Galois .gr, or MatrixMarket with
+    fmt="market"); returns its edge list as (src, dst, weights or None) arrays
+    in output order."""
     b = lambda x: "true" if x else "false"
-    subprocess.run([REF_GTOOLS, f"--graphfile={gr_path}", "--format=gr", f"--output={out_path}",
+    subprocess.run([REF_GTOOLS, f"--graphfile={gr_path}", f"--format={fmt}", f"--output={out_path}",
                     f"--deself_cycle={b(deself_cycle)}", f"--deduplicate={b(deduplicate)}", f"--d2ud={b(d2ud)}"],
                    check=True, capture_output=True)
     rows = np.loadtxt(out_path, dtype=np.int64, ndmin=2) if os.path.getsize(out_path) else np.zeros((0, 2))

@@ -342,6 +342,96 @@ sg_status write_gr(const HostGraph &g, const char *path) {
     return ok ? SG_OK : SG_ERR_IO;
 }
 
+// METIS graph file (ReadGraph, src/utils/parser.cpp:230-396): '%' comment
+// lines are skipped; the header is "n m [fmt [ncon]]" with m counting every
+// undirected edge once; fmt's digits select vertex sizes, vertex weights
+// (ncon per vertex, ncon > 0 only with vertex weights) and edge weights;
+// vertex i's line lists 1-based neighbours, each followed by its positive
+// weight when edge weights are present, in file order (no sorting or
+// deduplication); exactly 2m entries must be listed.  Vertex sizes and
+// weights are read and dropped (the engine has no use for them).  The
+// reference scans the header with a 64-bit conversion into 32-bit fields
+// (parser.h SCIDX); the header is read here as the format defines it.
+sg_status read_metis(const char *path, HostGraph &g) {
+    FILE *f = std::fopen(path, "r");
+    if (!f) return SG_ERR_IO;
+    std::string line;
+    auto next_line = [&]() -> bool {
+        do {
+            line.clear();
+            int c;
+            bool any = false;
+            while ((c = std::fgetc(f)) != EOF) {
+                any = true;
+                if (c == '\n') break;
+                line.push_back((char)c);
+            }
+            if (!any) return false;
+        } while (!line.empty() && line[0] == '%');
+        return true;
+    };
+    auto fail = [&](sg_status st) {
+        std::fclose(f);
+        return st;
+    };
+    unsigned long long n = 0, m = 0, fmt = 0, ncon = 0;
+    if (!next_line()) return fail(SG_ERR_FORMAT);
+    const int fields = std::sscanf(line.c_str(), "%llu %llu %llu %llu", &n, &m, &fmt, &ncon);
+    if (fields < 2 || n == 0 || m == 0 || n >= (1ull << 32) || 2 * m >= (1ull << 32) || fmt > 111)
+        return fail(SG_ERR_FORMAT);
+    const bool readvs = (fmt / 100) % 10 == 1, readvw = (fmt / 10) % 10 == 1, readew = fmt % 10 == 1;
+    if (ncon > 0 && !readvw) return fail(SG_ERR_FORMAT);
+    if (ncon == 0) ncon = 1;
+    const uint64_t ne = 2 * m;
+    g.nv = (uint32_t)n;
+    g.offsets.assign(n + 1, 0);
+    g.indices.clear();
+    g.weights.clear();
+    try {
+        g.indices.reserve(ne);
+        if (readew) g.weights.reserve(ne);
+    } catch (...) {
+        return fail(SG_ERR_OUT_OF_MEMORY);
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        if (!next_line()) return fail(SG_ERR_FORMAT);
+        const char *cur = line.c_str();
+        char *end = nullptr;
+        if (readvs) {
+            const long long vs = std::strtoll(cur, &end, 10);
+            if (end == cur || vs < 0) return fail(SG_ERR_FORMAT);
+            cur = end;
+        }
+        if (readvw) {
+            for (uint64_t l = 0; l < ncon; ++l) {
+                const long long vw = std::strtoll(cur, &end, 10);
+                if (end == cur || vw < 0) return fail(SG_ERR_FORMAT);
+                cur = end;
+            }
+        }
+        for (;;) {
+            const long long e = std::strtoll(cur, &end, 10);
+            if (end == cur) break;
+            cur = end;
+            if (e < 1 || (unsigned long long)e > n) return fail(SG_ERR_FORMAT);
+            long long w = 1;
+            if (readew) {
+                w = std::strtoll(cur, &end, 10);
+                if (end == cur || w <= 0 || w >= (1ll << 32)) return fail(SG_ERR_FORMAT);
+                cur = end;
+            }
+            if (g.indices.size() == ne) return fail(SG_ERR_FORMAT);  // more entries than 2m
+            g.indices.push_back((uint32_t)(e - 1));
+            if (readew) g.weights.push_back((uint32_t)w);
+        }
+        g.offsets[i + 1] = (uint32_t)g.indices.size();
+    }
+    std::fclose(f);
+    if (g.indices.size() != ne) return SG_ERR_FORMAT;
+    g.ne = ne;
+    return SG_OK;
+}
+
 sg_status read_market(const char *path, bool symmetrize, HostGraph &g) {
     FILE *f = std::fopen(path, "r");
     if (!f) return SG_ERR_IO;

@@ -28,6 +28,7 @@ sg_status from_csr(uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint
 sg_status read_gr(const char *path, HostGraph &g);
 sg_status write_gr(const HostGraph &g, const char *path);
 sg_status read_market(const char *path, bool symmetrize, HostGraph &g);
+sg_status read_metis(const char *path, HostGraph &g);
 sg_status max_degree_vertex(const HostGraph &g, uint32_t *vertex, uint32_t *degree);
 sg_status pick_sources(const HostGraph &g, uint32_t n, uint64_t seed, uint32_t *out);
 }  // namespace sgb

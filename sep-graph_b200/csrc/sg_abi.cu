@@ -731,6 +731,19 @@ sg_status sg_hgraph_write_gr(const sg_hgraph *h, const char *path) {
     return sgb::write_gr(*h, path);
 }
 
+sg_status sg_hgraph_read_metis(const char *path, sg_hgraph **out) {
+    if (!path || !out) return SG_ERR_INVALID_ARG;
+    sg_hgraph *h = new (std::nothrow) sg_hgraph;
+    if (!h) return SG_ERR_OUT_OF_MEMORY;
+    sg_status st = sgb::read_metis(path, *h);
+    if (st != SG_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return SG_OK;
+}
+
 sg_status sg_hgraph_read_market(const char *path, int symmetrize, sg_hgraph **out) {
     if (!path || !out) return SG_ERR_INVALID_ARG;
     sg_hgraph *h = new (std::nothrow) sg_hgraph;

@@ -206,6 +206,7 @@ def load() -> C.CDLL:
         "sg_hgraph_read_gr": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
         "sg_hgraph_write_gr": (C.c_int, [_P, C.c_char_p]),
         "sg_hgraph_read_market": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_P)]),
+        "sg_hgraph_read_metis": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
         "sg_hgraph_info": (C.c_int, [_P, _U32P, C.POINTER(C.c_uint64), C.POINTER(_U32P), C.POINTER(_U32P),
                                      C.POINTER(_U32P)]),
         "sg_hgraph_max_degree_vertex": (C.c_int, [_P, _U32P, _U32P]),
@@ -308,6 +309,12 @@ class HostGraph:
     def read_market(cls, path: str, symmetrize: bool = False) -> "HostGraph":
         h = _P()
         _check(load().sg_hgraph_read_market(path.encode(), int(symmetrize), C.byref(h)), "read_market")
+        return cls(h)
+
+    @classmethod
+    def read_metis(cls, path: str) -> "HostGraph":
+        h = _P()
+        _check(load().sg_hgraph_read_metis(path.encode(), C.byref(h)), "read_metis")
         return cls(h)
 
     def write_gr(self, path: str):

@@ -206,3 +206,35 @@ def test_device_inputs(ctx):
     got = G.copy_out()
     G.close()
     assert _same(got, oracle.gtools_build(500, s, d, None, False, True, False, sort_rows=True))
+
+
+BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "sep-graph_b200", "bin")
+
+
+@pytest.mark.parametrize("path", CONVERT, ids=[os.path.basename(p)[:-4] for p in CONVERT])
+def test_gtools_cli_matches_reference_output(path, tmp_path):
+    """bin/gtools (the converter's flags and text outputs, preprocessing on the GPU)
+    on the golden edge lists: same edge list as the reference converter, and the
+    out-degree file agrees with it."""
+    import subprocess
+
+    exe = os.path.join(BIN, "gtools")
+    if not os.path.exists(exe):
+        pytest.skip("samples not built")
+    g = _load(path)
+    nv, w = int(g["nv"]), g.get("weights")
+    gr = str(tmp_path / "g.gr")
+    sg.HostGraph.from_csr(*_stable_csr(nv, g["src"], g["dst"], w)).write_gr(gr)
+    b = lambda x: "true" if x else "false"
+    for code in range(8):
+        out, deg = str(tmp_path / "e.txt"), str(tmp_path / "d.txt")
+        r = subprocess.run([exe, f"--graphfile={gr}", f"--output={out}", f"--out_degree={deg}",
+                            f"--deself_cycle={b(code & 1)}", f"--deduplicate={b(code & 2)}", f"--d2ud={b(code & 4)}"],
+                           capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        rows = np.loadtxt(out, dtype=np.int64, ndmin=2) if os.path.getsize(out) else np.zeros((0, 3 if w is not None else 2))
+        assert np.array_equal(rows[:, 0], g[f"g{code}_src"]) and np.array_equal(rows[:, 1], g[f"g{code}_dst"]), code
+        if w is not None:
+            assert np.array_equal(rows[:, 2], g[f"g{code}_w"]), code
+        d = np.loadtxt(deg, dtype=np.int64, ndmin=2)
+        assert np.array_equal(d[:, 1], np.bincount(g[f"g{code}_src"].astype(np.int64), minlength=nv)), code

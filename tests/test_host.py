@@ -7,6 +7,7 @@ import subprocess
 import numpy as np
 import pytest
 
+import oracle
 import sepgraph as sg
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -180,6 +181,24 @@ SAMPLE_FLAGS = {
 }
 
 
+GTOOLS_FLAGS = {"graphfile", "ggr", "output", "out_degree", "splitter", "deself_cycle", "deduplicate", "format",
+                "d2ud"}  # samples/tools/gtools.cpp:15-23
+
+
+def test_gtools_flag_surface():
+    exe = os.path.join(BIN, "gtools")
+    if not os.path.exists(exe):
+        pytest.skip("samples not built")
+    out = subprocess.run([exe, "--help"], capture_output=True, text=True, timeout=30)
+    assert out.returncode == 0
+    names = set(re.findall(r"^\s+--(\w+)", out.stdout, re.M))
+    assert not GTOOLS_FLAGS - names, GTOOLS_FLAGS - names
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=30)
+    assert out.returncode == 0 and "A Graph File must be provided" in out.stdout
+    bad = subprocess.run([exe, "--no_such_flag=1"], capture_output=True, text=True, timeout=30)
+    assert bad.returncode != 0
+
+
 @pytest.mark.parametrize("sample", sorted(SAMPLE_FLAGS))
 def test_cli_flag_surface(sample):
     exe = os.path.join(BIN, sample)
@@ -211,3 +230,52 @@ def test_options_defaults_match_reference_flags():
     assert o.non_atomic == 1  # hybrid_bfs main.cpp:37
     assert abs(o.pr_error - 0.01) < 1e-12  # hybrid_pr main.cpp:37
     assert o.variant == -1 and o.lb_push == -1 and o.blocking == 1
+
+
+def _write(p, text):
+    p.write_text(text)
+    return str(p)
+
+
+def test_metis_reader(tmp_path):
+    """ReadGraph (src/utils/parser.cpp:230-396): comments, 1-based lists in file
+    order, m counted once per undirected edge, fmt digits for vertex sizes /
+    vertex weights (ncon) / edge weights, empty lines for isolated vertices."""
+    h = sg.HostGraph.read_metis(_write(tmp_path / "a.graph", "% c\n4 3\n3 2\n1\n1 4\n% mid\n3\n"))
+    assert h.offsets.tolist() == [0, 2, 3, 5, 6] and h.indices.tolist() == [2, 1, 0, 0, 3, 2]
+    assert h.weights is None
+    h = sg.HostGraph.read_metis(_write(tmp_path / "b.graph", "3 2 1\n2 7 3 9\n1 7\n1 9\n"))
+    assert h.indices.tolist() == [1, 2, 0, 0] and h.weights.tolist() == [7, 9, 7, 9]
+    h = sg.HostGraph.read_metis(_write(tmp_path / "c.graph", "3 1 111 2\n5 1 2 2 4\n6 3 4 1 4\n0 1 1\n"))
+    assert h.offsets.tolist() == [0, 1, 2, 2] and h.indices.tolist() == [1, 0] and h.weights.tolist() == [4, 4]
+    h = sg.HostGraph.read_metis(_write(tmp_path / "d.graph", "3 1\n\n3\n2\n"))
+    assert h.offsets.tolist() == [0, 0, 1, 2] and h.indices.tolist() == [2, 1]
+    for bad in ("3 2\n2\n1\n\n",          # fewer entries than 2m
+                "2 1\n2 2\n1\n",           # more entries than 2m
+                "2 1\n3\n1\n",             # neighbour out of range
+                "2 1 112\n2\n1\n",         # unknown fmt
+                "2 1 1 2\n2 1\n1 1\n",     # ncon without vertex weights
+                "2 1 1\n2 0\n1 0\n",       # edge weight must be positive
+                "0 1\n"):
+        with pytest.raises(sg.SGError):
+            sg.HostGraph.read_metis(_write(tmp_path / "bad.graph", bad))
+
+
+@pytest.mark.skipif(not oracle.ref_gtools_available(), reason="reference converter not compiled here")
+@pytest.mark.parametrize("weighted", [False, True])
+def test_market_reader_matches_reference(tmp_path, weighted):
+    """Our MatrixMarket reader against the reference's ReadGraphMarket, read through
+    the reference converter with --deduplicate=false (it prints the CSR as read)."""
+    rng = np.random.default_rng(3 + weighted)
+    n, m = 60, 500
+    s, d = rng.integers(1, n + 1, m), rng.integers(1, n + 1, m)
+    w = rng.integers(1, 20, m)
+    lines = ["%%MatrixMarket matrix coordinate integer general", f"{n} {n} {m}"]
+    lines += [f"{a} {b} {c}" if weighted else f"{a} {b}" for a, b, c in zip(s, d, w)]
+    path = _write(tmp_path / "g.mtx", "\n".join(lines) + "\n")
+    rs, rd, rw = oracle.ref_gtools(path, str(tmp_path / "o.txt"), deduplicate=False, fmt="market")
+    h = sg.HostGraph.read_market(path)
+    src = np.repeat(np.arange(h.nv, dtype=np.uint32), np.diff(h.offsets.astype(np.int64)))
+    assert np.array_equal(src, rs) and np.array_equal(h.indices, rd)
+    if weighted:
+        assert np.array_equal(h.weights, rw)
