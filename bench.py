@@ -63,7 +63,7 @@ def args_parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--quick", action="store_true", help="headline line only")
     p.add_argument("--served-queries", type=int, default=1000)
-    p.add_argument("--extras", default="per_algo,batched,served,ingest", help="extra sections at N=1 (comma list)")
+    p.add_argument("--extras", default="per_algo,batched,ingest,served", help="extra sections at N=1 (comma list)")
     p.add_argument("--scale", type=int, default=SCALE)
     p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc"],
                    help="run one warm-up and one measured solve of that kernel only (for ncu captures)")
@@ -399,7 +399,7 @@ def run_ours(a):
         extra = {}
         cache = {"rmat22": (h, G)}
         wanted = set(a.extras.split(","))
-        for name, fn in (("per_algo", per_algo), ("batched", batched), ("served", served), ("ingest", ingest)):
+        for name, fn in (("per_algo", per_algo), ("batched", batched), ("ingest", ingest), ("served", served)):
             if name not in wanted:
                 continue
             t0 = time.perf_counter()

@@ -114,6 +114,10 @@ struct AppBase {
     common::MsgPassing m_msg_passing = common::MsgPassing::PUSH;
     common::Scheduling m_scheduling = common::Scheduling::DATA_DRIVEN;
     uint32_t *m_p_current_round = nullptr;
+    // Extension (no reference counterpart): set by the engine while local
+    // lookahead runs, when CombineValueBuffer may be called for one vertex by
+    // two blocks at once; reorder-safe functors then combine atomically.
+    bool m_concurrent_combine = false;
 
     __forceinline__ __device__ virtual TValue GetInitValue(index_t node) const = 0;
     __forceinline__ __device__ virtual TBuffer GetInitBuffer(index_t node) const = 0;

@@ -39,7 +39,11 @@ struct BFS : AppBase<TValue, TBuffer, TWeight> {
         TBuffer buf = *p_buffer;
         const bool improved = *p_value > buf;
         if (improved) {
-            *p_value = buf;
+            // under local lookahead two blocks may combine one vertex at once:
+            // the value then only moves down (a reduction, no read-back; a
+            // combine that saw a stale value expands once more, harmlessly)
+            if (this->m_concurrent_combine) atomicMin(p_value, buf);
+            else *p_value = buf;
             buf += 1;  // level offered to the neighbours
         }
         bool schedule;
@@ -95,7 +99,12 @@ struct SSSP : AppBase<TValue, TBuffer, TWeight> {
                                                                             TBuffer *p_buffer) override {
         const TBuffer buf = *p_buffer;
         const bool improved = *p_value > buf;
-        if (improved) *p_value = buf;
+        if (improved) {
+            // concurrent combines of one vertex (local lookahead) keep the
+            // smallest distance: a reduction without read-back
+            if (this->m_concurrent_combine) atomicMin(p_value, buf);
+            else *p_value = buf;
+        }
         const bool schedule = this->m_msg_passing == MsgPassing::PUSH ? improved : true;
         return utils::pair<TBuffer, bool>(buf, schedule);
     }
@@ -137,7 +146,9 @@ struct PageRank : AppBase<TValue, TBuffer, TWeight> {
                                                                             TBuffer *p_buffer) override {
         TBuffer res = atomicExch(p_buffer, (TBuffer)0.0f);
         if (res > 0) {
-            *p_value += res;
+            // two blocks may combine one vertex at once (local lookahead)
+            if (this->m_concurrent_combine) atomicAdd(p_value, res);
+            else *p_value += res;
             const index_t deg = this->m_msg_passing == MsgPassing::PUSH
                                     ? this->m_csr_graph.end_edge(node) - this->m_csr_graph.begin_edge(node)
                                     : this->m_csc_graph.out_degree(node);

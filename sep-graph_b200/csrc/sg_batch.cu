@@ -680,16 +680,21 @@ sg_status prepare_batch(sg_ctx *ctx, sgb::Workspace &ws, std::vector<engine::Bat
     // Automatic team size.  Equal teams claim queries largest first, so the
     // batch lasts at least as long as its largest query on one team: a team
     // gets 4x its edge-proportional share of the grid, blocks * 4 * ne_max /
-    // sum(ne), and at least one block per 2M edges of the largest graph.
-    // Measured on B200 (592 blocks): 256 SSSP queries over RMAT scales 12-20
-    // ran in 27-30 ms with 24-49 blocks per team against 72 ms with 7; 256 on
-    // RMAT-14 fastest with 8-10; 64 BFS on RMAT-22 flat from 24 to 148.
+    // sum(ne), and at least one block per 2M edges of the largest graph; but
+    // the grid keeps at least min(n, 16) teams, because queries on
+    // high-diameter graphs are bound by their round count, not their edges,
+    // and gain from running side by side.  Measured on B200 (592 blocks): 256
+    // SSSP queries over RMAT scales 12-20 ran in 27-30 ms with 24-49 blocks
+    // per team against 72 ms with 7; 256 on RMAT-14 fastest with 8-10; 64 BFS
+    // on RMAT-22 flat from 24 to 148; mixed RMAT/grid server batches lost half
+    // their throughput with one or two large teams.
     uint32_t team_blocks = (uint32_t)o.team_blocks;
     if (o.team_blocks <= 0) {
         uint64_t sum_ne = 0;
         for (auto *g : graphs) sum_ne += g->ne;
         const uint64_t share = (4ull * total_blocks * ne_max + sum_ne - 1) / std::max<uint64_t>(1, sum_ne);
-        team_blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(std::max(ne_max >> 21, share), total_blocks));
+        const uint64_t cap = std::max<uint64_t>(1, total_blocks / std::min(n, 16u));
+        team_blocks = (uint32_t)std::max<uint64_t>(1, std::min(std::max(ne_max >> 21, share), cap));
     }
     team_blocks = std::max(1u, std::min(team_blocks, total_blocks));
     const uint32_t n_teams = std::max(1u, std::min(n, total_blocks / team_blocks));

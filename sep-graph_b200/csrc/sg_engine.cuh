@@ -242,6 +242,13 @@ struct has_pull_reduce<App, TB,
 // pull round, whose frontier must already hold every vertex those chunks would
 // reach, and level-synchronous functors (BC's path counting) need both halves
 // of a round apart, so both keep the barrier.
+// Local lookahead (Params::local_depth) also relies on this declaration, and
+// adds one obligation: a block may combine a vertex it discovered while
+// another block combines the same vertex (from its own lookahead queue or the
+// round's worklist), so a reorder-safe functor's CombineValueBuffer must
+// tolerate concurrent calls for one vertex while m_concurrent_combine is set
+// (BFS/SSSP: atomic minimum on the value; PageRank: atomic exchange of the
+// residual, atomic add to the value).
 template <typename App, typename = void>
 struct has_reorder_safe : std::false_type {};
 template <typename App>
@@ -1292,6 +1299,8 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         const int var = s.variant;
         const uint32_t set = s.round & 1u;  // heavy-vertex table this round registers into
         K::set_app_variant(app, var);
+        app.m_concurrent_combine =
+            var == V_ASYNC_PUSH_DD && a.p.local_depth > 0 && a.p.forced == V_ASYNC_PUSH_DD && reorder_safe(app);
         if (s.chunks) {
             // chunks of the heavy vertices the previous push round found (reorder-safe functors only)
             K::heavy_phase(app, a, s, set ^ 1u, true, acc);
