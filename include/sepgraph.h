@@ -208,6 +208,15 @@ sg_status sg_msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint32_
 
 /* One query of a batch: graph (any graph of the context), source, and the
  * output array of graph->nv uint32 (host or device memory). */
+/* Multi-source BC: up to 32 sources of one graph in one launch (bit-parallel
+ * forward over in-edges, level-by-level backward); bc_out holds nsrc rows of
+ * nv floats (host or device), row i equal to sg_bc(g, sources[i]) within
+ * float summation order.  Needs the graph's in-edge view (CSC or
+ * SG_GRAPH_SYMMETRIC), else SG_ERR_UNSUPPORTED.  Device memory ~ 40 x nv x 32
+ * bytes of scratch.  No reference counterpart (one source per Engine). */
+sg_status sg_msbc(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt, float *bc_out,
+                  sg_stats *stats);
+
 typedef struct sg_batch_query {
     sg_graph *graph;
     uint32_t source;

@@ -162,6 +162,7 @@ def load() -> C.CDLL:
         "sg_graph_create": (C.c_int, [_P, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_uint32, C.POINTER(_P)]),
         "sg_graph_create_from_host": (C.c_int, [_P, _P, C.c_uint32, C.POINTER(_P)]),
         "sg_graph_destroy": (C.c_int, [_P]),
+        "sg_msbc": (C.c_int, [_P, _P, C.c_uint32, C.POINTER(Options), _P, C.POINTER(Stats)]),
         "sg_graph_build": (C.c_int, [_P, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
         "sg_graph_copy_out": (C.c_int, [_P, C.c_int, _P, _P, _P]),
         "sg_graph_info": (C.c_int, [_P, _U32P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
@@ -690,6 +691,17 @@ class Graph:
         st = Stats()
         _check(load().sg_msbfs(self._g, src.ctypes.data_as(_U32P), len(src), C.byref(o), _ptr(out), C.byref(st)),
                "sg_msbfs", self.ctx.handle)
+        return out, st
+
+    def msbc(self, sources, out=None, **opts):
+        """Betweenness centrality from up to 32 sources in one launch; returns (bc[nsrc, nv], stats)."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        o = make_options(**opts)
+        if out is None:
+            out = np.empty((len(src), self.nv), np.float32)
+        st = Stats()
+        _check(load().sg_msbc(self._g, src.ctypes.data, len(src), C.byref(o), _ptr(out), C.byref(st)),
+               "sg_msbc", self.ctx.handle)
         return out, st
 
     def bc(self, source: int, out=None, sigma_out=None, trace_capacity: int = 0, **opts):

@@ -172,3 +172,72 @@ def test_batch_plan_rejects_host_outputs(ctx, uneven_graphs):
     h, G = uneven_graphs[0]
     with pytest.raises(sg.SGError):
         ctx.batch_plan("bfs", [(G, 0)], [np.zeros(h.nv, np.uint32)])
+
+
+def _msbc_case(ctx, h, srcs, sym):
+    G = ctx.graph(h, symmetric=sym)
+    try:
+        rows, st = G.msbc(srcs, max_iteration=1000000)
+        assert st.device_error == 0
+        for i, s in enumerate(srcs):
+            single, _, _ = G.bc(int(s), max_iteration=1000000)
+            assert np.allclose(rows[i], single, rtol=1e-4, atol=1e-5), (i, s)
+            if h.nv <= 2048:
+                want, _, _ = oracle.bc_f64(h.offsets, h.indices, int(s))
+                assert np.allclose(rows[i], want, rtol=1e-4, atol=1e-4), (i, s)
+    finally:
+        G.close()
+
+
+@pytest.mark.parametrize("scale,sym,n", [(10, True, 32), (12, False, 32), (13, True, 7), (14, True, 1)])
+def test_msbc_rmat_matches_single(ctx, scale, sym, n):
+    """Each row of multi-source BC equals sg_bc from that source (1e-4 relative)
+    and the FP64 oracle on small graphs; directed graphs pull over the CSC."""
+    h = sg.HostGraph.rmat(scale, 8, symmetric=sym, seed=scale)
+    srcs = [int(s) for s in h.pick_sources(n, 70 + scale)]
+    _msbc_case(ctx, h, srcs, sym)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_msbc_golden(ctx, path):
+    """Small shapes (chain, star, grid, disconnected, self-loops and duplicate
+    edges, single vertex) with every vertex as a source (up to 32), duplicates
+    included."""
+    z = np.load(path)
+    h = sg.HostGraph.from_csr(z["offsets"], z["indices"])
+    srcs = [v % h.nv for v in range(min(32, h.nv + 2))]
+    _msbc_case(ctx, h, srcs, False)
+
+
+def test_msbc_split_hubs(ctx):
+    """Vertices above 4096 in- and out-edges are split into chunks in both passes:
+    a directed double star (hub -> 9000 leaves, leaves -> second hub) plus a ring."""
+    n = 9003
+    off, idx = [0], []
+    for v in range(n):
+        if v == 0:
+            idx += list(range(2, n))        # hub 0 -> every leaf
+        elif v == 1:
+            idx += [0]                      # hub 1 -> hub 0
+        else:
+            idx += [1, v + 1 if v + 1 < n else 2]  # leaf -> hub 1, leaf ring
+        off.append(len(idx))
+    h = sg.HostGraph.from_csr(np.array(off, np.uint32), np.array(idx, np.uint32))
+    srcs = [0, 1, 2, 5000, 9002] + [int(x) for x in np.random.default_rng(3).integers(0, n, 27)]
+    _msbc_case(ctx, h, srcs, False)
+
+
+def test_msbc_rejects_bad_input(ctx):
+    h = sg.HostGraph.rmat(8, 8, seed=1)
+    G = ctx.graph(h)
+    with pytest.raises(sg.SGError):
+        G.msbc([])
+    with pytest.raises(sg.SGError):
+        G.msbc(list(range(33)))
+    with pytest.raises(sg.SGError):
+        G.msbc([h.nv])
+    G.close()
+    G = ctx.graph(h, no_csc=True)
+    with pytest.raises(sg.SGError):
+        G.msbc([0])
+    G.close()
