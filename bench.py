@@ -588,9 +588,13 @@ def batched(ctx, cache, a):
         plain.append(bc)
     ms_b, (outs, st_b, _) = _median_ms(lambda: ctx.bc_batch([(G, s) for s in srcs32]), 3)
     same_b = all(np.allclose(o, p, rtol=1e-4, atol=1e-5) for o, p in zip(outs, plain))
+    ms_mb, (rows_mb, _) = _median_ms(lambda: G.msbc(srcs32), 3)
+    same_mb = all(np.allclose(rows_mb[i], plain[i], rtol=1e-4, atol=1e-5) for i in range(len(srcs32)))
     res["bc32_rmat22_sym"] = {"plain_ms": plain_ms, "plain_qps": 32 / (plain_ms * 1e-3), "batch_ms": ms_b,
                               "batch_qps": 32 / (ms_b * 1e-3), "same_results_rtol_1e-4": same_b,
-                              "batch_GTEPS": st_b.edges_reached / ms_b / 1e6}
+                              "batch_GTEPS": st_b.edges_reached / ms_b / 1e6,
+                              "msbc_ms": ms_mb, "msbc_qps": 32 / (ms_mb * 1e-3),
+                              "msbc_same_results_rtol_1e-4": same_mb}
     G.close()
     del h, plain, outs
 

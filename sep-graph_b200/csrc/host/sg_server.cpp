@@ -156,6 +156,9 @@ uint64_t sg_server::estimate(const std::vector<Pending> &b) const {
         for (auto &kv : per_graph)
             if (kv.second >= std::max(1u, cfg.msbfs_min))
                 bytes += graphs[kv.first].nv * (32 + 4 * std::min<uint64_t>(kv.second, 64));
+    if (algo == SG_QUERY_BC)  // multi-source BC scratch: 32 path counts, dependencies, q, masks, lists, rows
+        for (auto &kv : per_graph)
+            if (kv.second >= std::max(1u, cfg.msbfs_min)) bytes += graphs[kv.first].nv * 1000ull;
     return bytes;
 }
 
@@ -220,18 +223,44 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
             }
         }
     } else {
-        // BC: one batched launch (forward and backward per team); a query that
-        // also asks for path counts runs alone through sg_bc
+        // BC: several queries on one graph -> multi-source BC (32 sources per
+        // launch, each row straight to its query); the rest, and any group the
+        // multi-source kernel declines (no in-edge view, path-count overflow),
+        // -> one batched launch (forward and backward per team), which reports
+        // per-query statuses; a query that also asks for path counts runs alone
+        // through sg_bc
         std::vector<sg_batch_query> q;
         std::vector<size_t> in_batch;
+        std::map<uint32_t, std::vector<size_t>> by_graph;
         for (size_t i = 0; i < b.size(); ++i) {
             if (b[i].q.out2) {
                 sg_graph *gv = view(slot, b[i].q.graph_id);
                 status[i] = gv ? sg_bc(gv, b[i].q.source, &o, (float *)b[i].q.out, (uint64_t *)b[i].q.out2, nullptr)
                                : SG_ERR_OUT_OF_MEMORY;
             } else {
-                q.push_back({graphs[b[i].q.graph_id].g, b[i].q.source, 0, b[i].q.out});
-                in_batch.push_back(i);
+                by_graph[b[i].q.graph_id].push_back(i);
+            }
+        }
+        for (auto &kv : by_graph) {
+            sg_graph *gv = kv.second.size() >= std::max(1u, cfg.msbfs_min) ? view(slot, kv.first) : nullptr;
+            for (size_t s = 0; s < kv.second.size(); s += 32) {
+                const size_t m = std::min<size_t>(32, kv.second.size() - s);
+                bool ok = false;
+                if (gv) {
+                    std::vector<uint32_t> src(m);
+                    std::vector<float *> rows(m);
+                    for (size_t k = 0; k < m; ++k) {
+                        src[k] = b[kv.second[s + k]].q.source;
+                        rows[k] = (float *)b[kv.second[s + k]].q.out;
+                    }
+                    ok = sgb::msbc_rows(gv, src.data(), (uint32_t)m, &o, nullptr, rows.data(), nullptr) == SG_OK;
+                }
+                if (ok) continue;
+                for (size_t k = 0; k < m; ++k) {
+                    const size_t i = kv.second[s + k];
+                    q.push_back({graphs[b[i].q.graph_id].g, b[i].q.source, 0, b[i].q.out});
+                    in_batch.push_back(i);
+                }
             }
         }
         if (!q.empty())

@@ -13,6 +13,10 @@ namespace sgb {
 sg_status msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt,
                    uint32_t *levels_out, sg_stats *stats, uint32_t *const *row_outs = nullptr);
 
+// Multi-source BC (<= 32 sources) with row i written to row_outs[i] (host or
+// device, nv floats each) when row_outs is given, else to bc_out.
+sg_status msbc_rows(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt, float *bc_out,
+                    float *const *row_outs, sg_stats *stats);
 // The context a graph was created on.
 sg_ctx *graph_context(const sg_graph *g);
 // Sum of the graph's edge weights (its edge count when unweighted).

@@ -402,9 +402,14 @@ __global__ void __launch_bounds__(kMbThreads) msbc_kernel(MbArgs a) {
 
 }  // namespace
 
-extern "C" sg_status sg_msbc(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt,
-                             float *bc_out, sg_stats *stats) {
-    if (!g || !g->ctx || !sources || !bc_out || nsrc == 0 || nsrc > kMbSources) return SG_ERR_INVALID_ARG;
+namespace sgb {
+
+// Multi-source BC into bc_out (nsrc rows of nv) or, when row_outs is given,
+// row i to row_outs[i] (host or device, nv floats each).
+sg_status msbc_rows(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt, float *bc_out,
+                    float *const *row_outs, sg_stats *stats) {
+    if (!g || !g->ctx || !sources || (!bc_out && !row_outs) || nsrc == 0 || nsrc > kMbSources)
+        return SG_ERR_INVALID_ARG;
     sg_ctx *ctx = g->ctx;
     for (uint32_t i = 0; i < nsrc; ++i)
         if (sources[i] >= g->nv) return sgb::set_error(ctx, SG_ERR_INVALID_ARG, "source %u out of range", sources[i]);
@@ -442,7 +447,7 @@ extern "C" sg_status sg_msbc(sg_graph *g, const uint32_t *sources, uint32_t nsrc
     SG_TRY_CUDA(ctx, ws.get("mb_sources", kMbSources, &dsrc));
     SG_TRY_CUDA(ctx, cudaMemcpyAsync(dsrc, sources, 4 * nsrc, cudaMemcpyHostToDevice, ctx->stream));
     a.sources = dsrc;
-    const bool out_dev = sgb::is_device_ptr(bc_out, ctx->device);
+    const bool out_dev = !row_outs && sgb::is_device_ptr(bc_out, ctx->device);
     if (out_dev) a.bc = bc_out;
     else SG_TRY_CUDA(ctx, ws.get("mb_bc", (size_t)nsrc * nv, &a.bc));
     a.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
@@ -471,7 +476,12 @@ extern "C" sg_status sg_msbc(sg_graph *g, const uint32_t *sources, uint32_t nsrc
         if (!(h.cnt.error & dev::kErrCapacity) || per == kMbSources) break;
     }
     SG_TRY_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    if (!out_dev) SG_TRY_CUDA(ctx, cudaMemcpy(bc_out, a.bc, 4ull * nsrc * nv, cudaMemcpyDeviceToHost));
+    if (row_outs) {
+        for (uint32_t i = 0; i < nsrc; ++i)
+            SG_TRY_CUDA(ctx, cudaMemcpy(row_outs[i], a.bc + (size_t)i * nv, 4ull * nv, cudaMemcpyDefault));
+    } else if (!out_dev) {
+        SG_TRY_CUDA(ctx, cudaMemcpy(bc_out, a.bc, 4ull * nsrc * nv, cudaMemcpyDeviceToHost));
+    }
     const uint32_t bits = h.cnt.error;
     if (stats) {
         std::memset(stats, 0, offsetof(sg_stats, trace));
@@ -483,4 +493,12 @@ extern "C" sg_status sg_msbc(sg_graph *g, const uint32_t *sources, uint32_t nsrc
     const sg_status st = sgb::device_error_status(bits);
     if (st != SG_OK) return sgb::set_error(ctx, st, "multi-source BC device error bits 0x%x", bits);
     return SG_OK;
+}
+
+}  // namespace sgb
+
+extern "C" sg_status sg_msbc(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const sg_options *opt,
+                             float *bc_out, sg_stats *stats) {
+    if (!bc_out) return SG_ERR_INVALID_ARG;
+    return sgb::msbc_rows(g, sources, nsrc, opt, bc_out, nullptr, stats);
 }

@@ -171,7 +171,38 @@ def test_low_load_grid_sssp_matches_alone():
         assert all(st == 0 for st in sts)
         for (al, g, s), got in zip(qs, outs):
             G = graphs[g][1]
-            want = G.sssp(s, variant="async_push_dd", max_iteration=1000000)[0] if al == "sssp" else G.bfs(s)[0]
+            want = (G.sssp(s, variant="async_push_dd", max_iteration=1000000)[0] if al == "sssp"
+                    else G.bfs(s, max_iteration=1000000)[0])
             assert np.array_equal(got, want), (al, g, s, int((got != want).sum()))
+    finally:
+        ctx.close()
+
+
+def test_bc_groups_match_alone():
+    """BC queries that share a graph run as multi-source launches (32 per
+    launch); a graph without an in-edge view falls back to the team batch.
+    Every result must equal sg_bc from that source."""
+    ctx = sg.Context(0)
+    try:
+        specs = [(sg.HostGraph.rmat(12, 8, symmetric=True, seed=41), dict(symmetric=True)),
+                 (sg.HostGraph.rmat(11, 8, seed=42), {}),
+                 (sg.HostGraph.rmat(11, 8, seed=43), dict(no_csc=True))]
+        graphs = [(h, ctx.graph(h, **kw)) for h, kw in specs]
+        rng = random.Random(9)
+        qs = [(g, int(graphs[g][0].pick_sources(1, rng.randrange(1 << 30))[0])) for g in (0,) * 40 + (1,) * 20 + (2,) * 8]
+        outs = [np.zeros(graphs[g][0].nv, np.float32) for g, _ in qs]
+        srv = sg.Server(0, slots=2, max_batch=256)
+        try:
+            for _, G in graphs:
+                srv.add_graph(G)
+            tickets = [srv.submit("bc", g, s, outs[i]) for i, (g, s) in enumerate(qs)]
+            sts = [srv.wait(t, 600.0)[0] for t in tickets]
+        finally:
+            srv.close()
+        assert all(st == 0 for st in sts), sts
+        for (g, s), got in zip(qs, outs):
+            # the graph without an in-edge view runs push-only, as the batch does
+            want = graphs[g][1].bc(s, variant="async_push_dd" if g == 2 else None)[0]
+            assert np.allclose(got, want, rtol=1e-4, atol=1e-5), (g, s)
     finally:
         ctx.close()
