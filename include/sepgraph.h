@@ -79,7 +79,8 @@ typedef struct sg_options {
     int32_t lb_pull;          /* SetLoadBalancing(PULL, ..) */
     int32_t priority;         /* SG_PRIORITY_NONE / LOW_HIGH (SetTwoLevelBasedPriority) */
     double priority_delta;    /* two-level priority step; <=0 with LOW_HIGH = auto (32*avg_w/avg_deg) */
-    double cut_threshold;     /* SetSampleBasedPriority (accepted, see DESIGN) */
+    double cut_threshold;     /* with SG_PRIORITY_SAMPLING: SetSampleBasedPriority; each ASYNC_PUSH_TD round
+                                 takes the vertices above the buffer value at 1000*(1-cut) of 1000 sampled */
     double alpha;             /* --alpha (15) */
     double beta;              /* --beta (18) */
     double edge_factor;       /* --edge_factor (1.0) */

@@ -46,7 +46,10 @@ static bool HybridPageRank() {
     if (!LoadGraph(g)) return false;
     sg_options o = CommonOptions();
     o.pr_error = FLAGS_error;
-    if (FLAGS_cut_threshold > 0) o.cut_threshold = FLAGS_cut_threshold;
+    if (FLAGS_cut_threshold > 0) {  // engine_opt.SetSampleBasedPriority (hybrid_pr.cu:135-137)
+        o.priority = SG_PRIORITY_SAMPLING;
+        o.cut_threshold = FLAGS_cut_threshold;
+    }
     if (FLAGS_sparse) {
         o.lb_push = SG_LB_NONE;
         o.lb_pull = SG_LB_NONE;

@@ -939,6 +939,7 @@ engine::Params batch_params(const sg_options &o, int scheme) {
     p.chunk_edges = o.chunk_edges > 0 ? (uint32_t)std::max(32, o.chunk_edges) : 256u;
     p.pull_warp_threshold = 32;
     p.local_depth = o.local_depth > 0 ? (uint32_t)o.local_depth : 0u;
+    p.sample_cut = o.priority == SG_PRIORITY_SAMPLING && o.cut_threshold > 0 ? (float)std::min(o.cut_threshold, 1.0) : 0.f;
     p.alpha = o.alpha;
     p.beta = o.beta > 0 ? o.beta : 18;
     p.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);

@@ -33,6 +33,7 @@
 // overflow silently, graph_datum.cuh:90).
 #pragma once
 #include <cstdint>
+#include <limits>
 #include <cstring>
 #include <type_traits>
 #include <utility>
@@ -118,6 +119,7 @@ struct Params {
     uint32_t chunk_edges;
     uint32_t pull_warp_threshold;
     uint32_t local_depth;  // levels a block follows its own discoveries inside a push round (0 = off)
+    float sample_cut;      // sampling priority in ASYNC_PUSH_TD rounds (SetSampleBasedPriority), 0 = off
     double alpha, beta;
     long long total_workload0;
     unsigned long long prio_init_raw, prio_step_raw;
@@ -656,6 +658,49 @@ struct EngineKernel {
 
     // ---------------------------------------------------------------- push
     // Phase A of a push round over worklist items (DD) or all vertices (TD).
+    // Sampling priority threshold (GetPriorityThreshold, algo_variants.cuh:98-131):
+    // the buffers of 1000 vertices drawn at random are sorted and the value at
+    // index 1000 * (1 - cut) becomes the round's threshold.  The reference draws
+    // with the unseeded std::rand; here a counter-based hash of (round, index).
+    // Run by one block (all its threads) in `scratch` (1024 buffer values of
+    // shared memory that topology-driven rounds leave unused), which publishes
+    // the threshold in the control block's prio_raw.
+    static __device__ void sample_threshold(const Args &a, const Snap &s, TB *vals) {
+        constexpr uint32_t kSample = 1000, kPad = 1024;
+        const uint32_t nn = a.csr.nnodes;
+        const uint32_t n = min(kSample, nn);
+        for (uint32_t i = threadIdx.x; i < kPad; i += blockDim.x) {
+            TB x = std::numeric_limits<TB>::max();
+            if (i < n) {
+                unsigned long long h = ((unsigned long long)s.round << 32) ^ i ^ 0x9E3779B97F4A7C15ull;
+                h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
+                h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
+                h ^= h >> 31;
+                x = dev::ld_l2(a.buffer + (uint32_t)(h % nn));
+            }
+            vals[i] = x;
+        }
+        __syncthreads();
+        for (uint32_t k = 2; k <= kPad; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < kPad / 2; i += blockDim.x) {
+                    const uint32_t lo = ((i & ~(j - 1)) << 1) | (i & (j - 1)), hi = lo + j;
+                    const TB x = vals[lo], y = vals[hi];
+                    if ((x > y) == ((lo & k) == 0)) {
+                        vals[lo] = y;
+                        vals[hi] = x;
+                    }
+                }
+                __syncthreads();
+            }
+        if (threadIdx.x == 0) {
+            uint32_t idx = (uint32_t)((float)n * (1.0f - a.p.sample_cut));
+            if (idx >= n) idx = n - 1;
+            __stcg(&a.ctrl->rs.prio_raw, to_raw<TB>(vals[idx]));
+        }
+        __syncthreads();
+    }
+
     static __device__ void push_phase_a(App &app, const Args &a, const Snap &s, WarpLB<TB> &wlb, bool dd,
                                         int lb, Acc &acc, LocalQ *lq = nullptr) {
         const uint32_t lane = dev::lane_id();
@@ -671,6 +716,9 @@ struct EngineKernel {
             bool keep = false;
             if (valid) {
                 v = dd ? dev::ld_l2(Q + i) : i;
+                // sampling priority: a topology-driven round takes only the
+                // vertices above this round's sampled threshold (driver.cuh:362-383)
+                if (!dd && a.p.sample_cut > 0.f) proceed = app.App::IsHighPriority(prio, dev::ld_l2(a.buffer + v));
                 if (dd) {
                     dev::bitmap_clear(a.qflag[s.qin], v);  // pop
                     if (s.pile && !app.App::IsHighPriority(prio, dev::ld_l2(a.buffer + v))) {
@@ -1331,6 +1379,13 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
                 break;
             }
             case V_ASYNC_PUSH_TD: {
+                if (a.p.sample_cut > 0.f) {  // this round's threshold, from the team's first block
+                    static_assert(sizeof(LocalQ::item) >= 1024 * sizeof(TB), "sample scratch");
+                    if (g_team_rank == 0) K::sample_threshold(a, s, reinterpret_cast<TB *>(&lq_block.item[0][0]));
+                    if (!grid_sync(c, tmo, nop)) return false;
+                    if (threadIdx.x == 0) s.prio_raw = __ldcg(&a.ctrl->rs.prio_raw);
+                    __syncthreads();
+                }
                 K::clear_dirty(a, s);
                 K::release_input_flags(a, s, false);
                 K::push_phase_a(app, a, s, my_lb, false, lb_push, acc);

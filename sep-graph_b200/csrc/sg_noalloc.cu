@@ -178,6 +178,7 @@ extern "C" sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *ind
     p.chunk_edges = kChunkEdges;
     p.pull_warp_threshold = 32;
     p.local_depth = o.local_depth > 0 ? (uint32_t)o.local_depth : 0u;
+    p.sample_cut = 0.f;
     p.alpha = o.alpha;
     p.beta = o.beta > 0 ? o.beta : 18;
     p.total_workload0 = (long long)((double)ne * (o.edge_factor > 0 ? o.edge_factor : 1.0));

@@ -181,6 +181,7 @@ struct EngineConfig {
     uint32_t heavy_degree = 32;  // out/in-degree above which a vertex is split into chunks
     uint32_t chunk_edges = 256;
     uint32_t local_depth = 0;  // local lookahead levels in push rounds (0 = off)
+    float sample_cut = 0.f;    // sampling priority cut in ASYNC_PUSH_TD rounds (0 = off)
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -286,6 +287,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     p.chunk_edges = chunk_edges;
     p.pull_warp_threshold = 32;
     p.local_depth = cfg.local_depth;
+    p.sample_cut = cfg.sample_cut;
     p.alpha = cfg.alpha;
     p.beta = cfg.beta;
     p.total_workload0 = (long long)((double)ne * cfg.edge_factor);
@@ -401,6 +403,7 @@ class Engine {
                           ? (int)m_opt.GetLoadBalancing(common::MsgPassing::PULL)
                           : (avg_deg >= 5 ? LB_FINE : LB_NONE);
         cfg.priority = m_opt.GetPriorityType() == common::Priority::LOW_HIGH;
+        if (m_opt.GetPriorityType() == common::Priority::SAMPLING) cfg.sample_cut = (float)m_opt.GetCutThreshold();
         cfg.prio_init_raw = to_raw<TBuffer>((TBuffer)m_opt.GetPriorityThreshold());
         cfg.prio_step_raw = cfg.prio_init_raw;
         cfg.max_iteration = max_iteration;

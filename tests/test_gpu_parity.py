@@ -146,6 +146,24 @@ def test_pagerank_rmat(ctx, variant):
     assert _pr_l1(r, ref64) <= PR_L1_TOL
 
 
+@pytest.mark.parametrize("cut", [0.05, 0.2, 1.0])
+def test_pagerank_sampling_priority(ctx, cut):
+    """SetSampleBasedPriority (--cut_threshold): each ASYNC_PUSH_TD round takes only
+    the vertices whose residual is at or above the sampled threshold; the fixed
+    point is unchanged (L1 against the FP64 oracle), and a small cut takes more
+    rounds than processing every vertex."""
+    h = sg.HostGraph.rmat(14, 16, symmetric=False, seed=1)
+    G = ctx.graph(h)
+    ref64 = oracle.pagerank_f64(h.offsets, h.indices, 1e-12)
+    r, st, _ = G.pagerank(variant="async_push_td", priority="sampling", cut_threshold=cut, pr_error=1e-7,
+                          max_iteration=100000)
+    assert _pr_l1(r, ref64) <= PR_L1_TOL, (cut, _pr_l1(r, ref64))
+    r0, st0, _ = G.pagerank(variant="async_push_td", pr_error=1e-7, max_iteration=100000)
+    if cut <= 0.05:
+        assert st.rounds > st0.rounds, (st.rounds, st0.rounds)
+    G.close()
+
+
 def test_bc_rmat(ctx):
     h = sg.HostGraph.rmat(14, 16, symmetric=True, seed=1)
     G = ctx.graph(h, symmetric=True)
