@@ -384,7 +384,7 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (graph arrays %.0f MB vs 126 MB L2)" % ((4 * (nv + 1) + 8 * ne) / 1e6),
                    "parallelism": f"replicas{world}"},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "what": "per step: pinned CSR+weights upload, 8 queries into pinned host distance arrays",
+                "what": "per step: pinned CSR+weights upload and device check into the graph arena the context kept from the previous step (sg_graph_destroy keeps it for reuse), 8 queries into pinned host distance arrays, graph released",
                 "ms_per_step": {k: 1e3 * v / e2e_steps for k, v in parts.items()}},
         "gpu_launches": a.steps * len(srcs),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -153,7 +153,14 @@ sg_status sg_device_info(sg_ctx *ctx, int *sm_count, uint64_t *hbm_bytes, uint64
 sg_status sg_graph_create(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *offsets, const uint32_t *indices,
                           const uint32_t *weights, uint32_t flags, sg_graph **out);
 sg_status sg_graph_create_from_host(sg_ctx *ctx, const sg_hgraph *h, uint32_t flags, sg_graph **out);
+/* The context keeps the arena of the last released graph (the larger one when
+ * several are released) and the next sg_graph_create / sg_graph_build whose
+ * graph needs between half of it and all of it reuses it, so reloading a graph
+ * costs no device allocation.  sg_ctx_release_cached frees that arena and the
+ * context's scratch of single-query and batched calls (reallocated on demand);
+ * sg_destroy frees everything. */
 sg_status sg_graph_destroy(sg_graph *g);
+sg_status sg_ctx_release_cached(sg_ctx *ctx);
 sg_status sg_graph_info(const sg_graph *g, uint32_t *nv, uint64_t *ne, uint64_t *device_bytes, int *weighted);
 
 /* Edge list -> device graph, built on the GPU.  Replaces the preprocessing of

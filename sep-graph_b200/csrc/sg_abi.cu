@@ -238,6 +238,7 @@ sg_status sg_destroy(sg_ctx *ctx) {
     DeviceGuard dg(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->spare_arena) cudaFree(ctx->spare_arena);
     delete ctx->batch_ws;
     delete ctx->graph_ws;
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -311,12 +312,20 @@ sg_status create_graph(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t *of
     g->weighted = weights != nullptr;
     g->symmetric = symmetric;
     g->has_csc = has_csc;
-    cudaError_t e = cudaMalloc(&g->arena, total);
-    if (e != cudaSuccess) {
-        delete g;
-        return sgb::cuda_status(ctx, e, "graph arena");
+    cudaError_t e = cudaSuccess;
+    if (ctx->spare_arena && ctx->spare_bytes >= total && ctx->spare_bytes / 2 <= total) {
+        g->arena = ctx->spare_arena;  // stream-ordered after the released graph's work
+        g->arena_bytes = ctx->spare_bytes;
+        ctx->spare_arena = nullptr;
+        ctx->spare_bytes = 0;
+    } else {
+        e = cudaMalloc(&g->arena, total);
+        if (e != cudaSuccess) {
+            delete g;
+            return sgb::cuda_status(ctx, e, "graph arena");
+        }
+        g->arena_bytes = total;
     }
-    g->arena_bytes = total;
     char *p = (char *)g->arena;
     auto carve = [&](size_t bytes) {
         uint32_t *q = (uint32_t *)p;
@@ -396,11 +405,35 @@ sg_status sg_graph_create_from_host(sg_ctx *ctx, const sg_hgraph *h, uint32_t fl
 
 sg_status sg_graph_destroy(sg_graph *g) {
     if (!g) return SG_ERR_INVALID_ARG;
-    DeviceGuard dg(g->ctx->device);
-    cudaStreamSynchronize(g->ctx->stream);
-    if (g->arena) cudaFree(g->arena);
-    g->ctx->live_graphs--;
+    sg_ctx *ctx = g->ctx;
+    DeviceGuard dg(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (g->arena) {
+        // keep the larger of this arena and the context's spare for the next graph
+        if (!ctx->spare_arena || ctx->spare_bytes < g->arena_bytes) {
+            if (ctx->spare_arena) cudaFree(ctx->spare_arena);
+            ctx->spare_arena = g->arena;
+            ctx->spare_bytes = g->arena_bytes;
+        } else {
+            cudaFree(g->arena);
+        }
+    }
+    ctx->live_graphs--;
     delete g;
+    return SG_OK;
+}
+
+sg_status sg_ctx_release_cached(sg_ctx *ctx) {
+    if (!ctx) return SG_ERR_INVALID_ARG;
+    DeviceGuard dg(ctx->device);
+    SG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->spare_arena) cudaFree(ctx->spare_arena);
+    ctx->spare_arena = nullptr;
+    ctx->spare_bytes = 0;
+    delete ctx->graph_ws;
+    ctx->graph_ws = nullptr;
+    delete ctx->batch_ws;
+    ctx->batch_ws = nullptr;
     return SG_OK;
 }
 

@@ -36,6 +36,10 @@ struct sg_ctx {
     int live_graphs = 0;  // sg_destroy refuses while graphs of this context exist
     sgb::Workspace *batch_ws = nullptr;  // scratch of batched launches (team workspaces)
     sgb::Workspace *graph_ws = nullptr;  // scratch of single-query calls, shared by the context's graphs
+    // the arena of the last released graph, reused by the next graph that fits
+    // (between half its size and its size): reloading a graph costs no cudaMalloc/cudaFree
+    void *spare_arena = nullptr;
+    size_t spare_bytes = 0;
 };
 
 namespace sgb {

@@ -156,6 +156,7 @@ def load() -> C.CDLL:
         "sg_ctx_set_stream": (C.c_int, [_P, _P]),
         "sg_ctx_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
         "sg_ctx_synchronize": (C.c_int, [_P]),
+        "sg_ctx_release_cached": (C.c_int, [_P]),
         "sg_last_error": (C.c_char_p, [_P]),
         "sg_device_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                      C.c_char_p, C.c_size_t]),
@@ -481,6 +482,10 @@ class Context:
         _check(load().sg_graph_build(self._c, nv, m, _ptr(src), _ptr(dst), _ptr(weights), bflags, gflags,
                                      C.byref(g)), "sg_graph_build", self._c)
         return Graph(self, g)
+
+    def release_cached(self):
+        """Frees the context's cached device memory (spare graph arena, call scratch)."""
+        _check(load().sg_ctx_release_cached(self._c), "sg_ctx_release_cached", self._c)
 
     def close(self):
         """Releases the context; graphs still open on it are released first."""

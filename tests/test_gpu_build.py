@@ -238,3 +238,29 @@ def test_gtools_cli_matches_reference_output(path, tmp_path):
             assert np.array_equal(rows[:, 2], g[f"g{code}_w"]), code
         d = np.loadtxt(deg, dtype=np.int64, ndmin=2)
         assert np.array_equal(d[:, 1], np.bincount(g[f"g{code}_src"].astype(np.int64), minlength=nv)), code
+
+
+def test_released_arena_is_reused(ctx):
+    """sg_graph_destroy keeps the graph's arena in its context; the next graph that
+    fits (half to all of it) reuses it, results unchanged; sg_ctx_release_cached
+    frees it."""
+    c = sg.Context(0)
+    try:
+        h = sg.HostGraph.rmat(12, 8, seed=5)
+        G = c.graph(h)
+        b1 = G.info()["device_bytes"]
+        G.close()
+        h2 = sg.HostGraph.rmat(12, 8, seed=6)  # a little smaller or larger, same scale
+        G = c.graph(h2)
+        if G.info()["ne"] * 2 >= h.indices.size:
+            assert G.info()["device_bytes"] >= b1 // 2
+        src = h2.max_degree_vertex()[0]
+        assert np.array_equal(G.bfs(src)[0], oracle.bfs(h2.offsets, h2.indices, src))
+        assert _same(G.copy_out(csc=True), oracle.csr_tocsc(h2.offsets, h2.indices, None))
+        G.close()
+        c.release_cached()
+        G = c.graph(sg.HostGraph.rmat(14, 8, seed=7))  # larger than the old arena: its own allocation
+        assert G.info()["device_bytes"] > b1
+        G.close()
+    finally:
+        c.close()
