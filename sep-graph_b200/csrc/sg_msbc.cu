@@ -11,11 +11,12 @@
 //
 // Forward, level d -> d+1 (pull over in-edges): a vertex that some source has
 // not reached ORs its in-neighbours' frontier masks; for the new bits the
-// warp sums the in-neighbours' path counts lane by lane (no atomics except on
-// split hubs).  Work is tiered by in-degree: a thread finds the new bits of a
+// warp sums the in-neighbours' path counts lane by lane, eight row loads in
+// flight (no atomics except on split hubs).  Work is tiered by in-degree: a
+// thread finds the new bits of a
 // vertex with <= 64 in-edges and its warp then sums the counts of those
 // vertices one at a time; vertices with more in-edges are listed once for a
-// warp each, and those above 1024 are split into 512-edge chunks whose
+// warp each, and those above 512 are split into 256-edge chunks whose
 // partial sums are added atomically.  The level's discoveries are appended
 // to a list as (vertex, mask) pairs.
 //
@@ -45,8 +46,8 @@ using engine::Ctrl;
 
 constexpr int kMbThreads = 256;
 constexpr uint32_t kMbThreadDeg = 64;  // in-degree up to this: a thread finds the new sources
-constexpr uint32_t kMbSplit = 1024;    // degree above this: split into chunks
-constexpr uint32_t kMbChunk = 512;     // edges per chunk (RMAT-22, 32 sources: 26.8 ms vs 30.9 with 4096/2048)
+constexpr uint32_t kMbSplit = 512;     // degree above this: split into chunks
+constexpr uint32_t kMbChunk = 256;     // edges per chunk
 constexpr uint32_t kMbSources = 32;
 
 struct MbArgs {
@@ -81,7 +82,7 @@ __device__ __forceinline__ void add_checked(unsigned long long &acc, unsigned lo
     acc = r;
 }
 
-constexpr int kMbGather = 4;  // row loads in flight per gather step
+constexpr int kMbGather = 8;  // row loads in flight per gather step
 
 // The next up to kMbGather set bits of the warp-uniform mask m (32 = none).
 __device__ __forceinline__ void take_bits(uint32_t &m, uint32_t (&j)[kMbGather]) {
