@@ -8,8 +8,8 @@
 // levels and build the next active list.  A vertex reached by several
 // sources in the same round is expanded once for all of them, so 64 BFSs cost
 // a few passes over the graph instead of 64.  Work is balanced in three tiers
-// by degree: a thread per vertex up to 32 edges, a warp per vertex up to 2048,
-// and 2048-edge chunks of bigger vertices (listed once per launch) spread over
+// by degree: a thread per vertex up to 32 edges, a warp per vertex up to 256,
+// and 256-edge chunks of bigger vertices (listed once per launch) spread over
 // all warps, so one hub never holds up a round.  The direction switch uses the
 // single-source engine's rule (scout count against the in-edges of vertices
 // some source has not reached yet / alpha, and beta for leaving pull,
@@ -37,7 +37,7 @@ using engine::Ctrl;
 
 constexpr int kMsThreads = 256;
 constexpr uint32_t kMsWarp = 32;     // vertices above this degree are scanned by a whole warp
-constexpr uint32_t kMsChunk = 2048;  // vertices above this degree are split into chunks of this many edges
+constexpr uint32_t kMsChunk = 256;   // vertices above this degree are split into chunks of this many edges
 
 struct MsArgs {
     const uint32_t *row, *col;    // CSR
