@@ -96,8 +96,8 @@ bool same(int algo, const Result &a, const Result &b, double pr_error) {
 }  // namespace
 
 // Staged search: the mode first, then, keeping the best so far, blocks per
-// SM, push load balancing, local lookahead depth (BFS/SSSP) and the
-// heavy-vertex split threshold.  Every candidate must reproduce the first
+// SM, push load balancing, local lookahead depth (BFS/SSSP), the
+// heavy-vertex split threshold and the chunk size of split vertices.  Every candidate must reproduce the first
 // candidate's result before its time counts.
 extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources, uint32_t nsrc, const sg_options *base,
                                  uint32_t max_candidates, sg_options *best, double *best_ms, sg_tune_entry *report,
@@ -197,6 +197,17 @@ extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources,
         sg_options c = cur;
         c.heavy_degree = 128;
         trial(c);
+    }
+    if (push_mode && algo != SG_QUERY_PAGERANK) {
+        // edges per chunk of a split vertex: smaller chunks spread a hub's
+        // first relaxations over more warps (SSSP on RMAT-22: 64 -> 4.02 ms,
+        // 256 -> 4.12, 1024 -> 4.69 per source)
+        const sg_options cur = *best;
+        for (int ce : {64, 128}) {
+            sg_options c = cur;
+            c.chunk_edges = ce;
+            trial(c);
+        }
     }
     if (best_ms) *best_ms = best_t;
     return SG_OK;

@@ -65,7 +65,8 @@ class TuneEntry(C.Structure):
     _fields_ = [("options", Options), ("ms", C.c_double), ("status", C.c_int32), ("pad", C.c_int32)]
 
 
-TUNED_FIELDS = ("variant", "blocks_per_sm", "heavy_degree", "priority", "priority_delta", "lb_push", "local_depth")
+TUNED_FIELDS = ("variant", "blocks_per_sm", "heavy_degree", "chunk_edges", "priority", "priority_delta", "lb_push",
+                "local_depth")
 VARIANT_NAMES = {-1: "auto", 0: "sync_push_td", 1: "sync_push_dd", 2: "sync_pull_td", 3: "sync_pull_dd",
                  4: "async_push_td", 5: "async_push_dd", 6: "async_pull_td", 7: "async_pull_dd"}
 
@@ -78,7 +79,7 @@ def options_dict(o: Options, fields=TUNED_FIELDS) -> dict:
         d.pop("priority")
         d.pop("priority_delta", None)
     elif "priority" in d:
-        d["priority"] = "low_high"
+        d["priority"] = {1: "low_high", 2: "sampling"}.get(d["priority"], d["priority"])
     return d
 
 
