@@ -114,8 +114,12 @@ struct SSSP : AppBase<TValue, TBuffer, TWeight> {
         if (buffer == kInf) return this->ACCUMULATE_FAILURE_CONTINUE;
         const TBuffer cand = buffer + weight;
         if (cand >= *p_buffer) return this->ACCUMULATE_FAILURE_CONTINUE;
-        return cand < atomicMin(p_buffer, cand) ? this->ACCUMULATE_SUCCESS_CONTINUE
-                                                : this->ACCUMULATE_FAILURE_CONTINUE;
+        // The buffer only moves down, so a minimum reduction without read-back
+        // is enough: the load above saw a larger value, hence the destination
+        // has to be (re)scheduled.  A concurrent smaller candidate makes this a
+        // redundant schedule of an already scheduled vertex, never a missed one.
+        atomicMin(p_buffer, cand);
+        return this->ACCUMULATE_SUCCESS_CONTINUE;
     }
 
     __forceinline__ __device__ bool IsActiveNode(index_t, TBuffer buffer) const override { return buffer != kInf; }
