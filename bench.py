@@ -85,7 +85,9 @@ def run_profile(a):
         if a.profile == "sssp_push":
             _, st, _ = G.sssp(src, variant="async_push_dd", max_iteration=100000)
         elif a.profile == "sssp_delta":
-            _, st, _ = G.sssp(src, priority="low_high", priority_delta=8, max_iteration=1000000)
+            # the headline's tuned options: delta-stepping, 4 blocks per SM, lookahead 16
+            _, st, _ = G.sssp(src, variant="async_push_dd", priority="low_high", priority_delta=4,
+                              blocks_per_sm=4, local_depth=16, max_iteration=1000000)
         elif a.profile == "bfs":
             _, st, _ = G.bfs(src)
         elif a.profile == "pr_pull":
