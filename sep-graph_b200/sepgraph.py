@@ -246,6 +246,17 @@ def _ptr(a) -> Optional[int]:
     raise TypeError(type(a))
 
 
+def _ptr32(a) -> Optional[int]:
+    """_ptr for arrays the library reads as 32-bit words (indices, weights)."""
+    if a is not None and not isinstance(a, int):
+        size = a.itemsize if isinstance(a, np.ndarray) else a.element_size()
+        if size != 4:
+            raise TypeError(f"expected 32-bit elements, got {getattr(a, 'dtype', type(a))}")
+        if hasattr(a, "is_contiguous") and not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+    return _ptr(a)
+
+
 def make_options(**kw) -> Options:
     o = Options()
     _check(load().sg_options_default(C.byref(o)), "sg_options_default")
@@ -461,7 +472,7 @@ class Context:
             nv = len(offsets) - 1
         if ne is None:
             ne = len(indices)
-        _check(load().sg_graph_create(self._c, nv, ne, _ptr(offsets), _ptr(indices), _ptr(weights), flags,
+        _check(load().sg_graph_create(self._c, nv, ne, _ptr32(offsets), _ptr32(indices), _ptr32(weights), flags,
                                       C.byref(g)), "graph_create", self._c)
         return Graph(self, g)
 
@@ -480,7 +491,7 @@ class Context:
                   | (BUILD_D2UD if d2ud else 0) | (BUILD_SORT_ROWS if sort_rows else 0))
         gflags = (GRAPH_SYMMETRIC if symmetric else 0) | (GRAPH_NO_CSC if no_csc else 0)
         g = _P()
-        _check(load().sg_graph_build(self._c, nv, m, _ptr(src), _ptr(dst), _ptr(weights), bflags, gflags,
+        _check(load().sg_graph_build(self._c, nv, m, _ptr32(src), _ptr32(dst), _ptr32(weights), bflags, gflags,
                                      C.byref(g)), "sg_graph_build", self._c)
         return Graph(self, g)
 
