@@ -296,9 +296,11 @@ def run_ours(a):
     dout = torch.empty(nv, dtype=torch.int32, device="cuda")
 
     # ---- options from the library's autotuner (sg_autotune: mode/delta, blocks
-    # per SM, load balancing, lookahead depth, heavy threshold; every candidate
-    # must reproduce the first one's distances), untimed
-    tuned, tuned_ms, report = G.autotune("sssp", srcs[:2], max_iteration=1000000)
+    # per SM, load balancing, lookahead depth, heavy threshold, chunk size;
+    # every candidate must reproduce the first one's distances), untimed, on
+    # four sources drawn apart from the measured ones
+    tune_srcs = [int(s) for s in h.pick_sources(4, 97)]
+    tuned, tuned_ms, report = G.autotune("sssp", tune_srcs, max_iteration=1000000)
     kw = dict(tuned, max_iteration=1000000)
     best = "{variant}{d}".format(variant=tuned["variant"], d=f"_delta{tuned['priority_delta']:g}"
                                  if "priority" in tuned else "")
