@@ -170,12 +170,54 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def make_graph(scale):
+def make_graph(scale, rank=0):
+    """The headline graph and the sources one rank runs: every rank holds the
+    whole graph (replicas) and answers its own independent sources; rank 0's
+    are the single-GPU run's."""
     import sepgraph as sg
 
     h = sg.HostGraph.rmat(scale, EDGE_FACTOR, 0.57, 0.19, 0.19, seed=1).gen_weights(1, 64, 2)
-    srcs = [int(s) for s in h.pick_sources(N_SOURCES, 3)]
-    return h, srcs
+    return h, replica_sources(h, rank)
+
+
+def replica_sources(h, rank):
+    return [int(s) for s in h.pick_sources(N_SOURCES, 3 if rank == 0 else 3 + 1000 * rank)]
+
+
+class Ranks:
+    """Replica bookkeeping over torch.distributed: a barrier, and the maximum
+    (device time) and sum (work) over ranks; single-process when world == 1."""
+
+    def __init__(self, world, device=None):
+        self.world = world
+        self.device = device  # tensors for the all-reduce live here (cuda for NCCL, cpu for gloo)
+
+    def barrier(self):
+        import torch
+
+        if self.world > 1:
+            torch.distributed.barrier()
+        if self.device is not None and self.device.type == "cuda":
+            torch.cuda.synchronize()
+
+    def _reduce(self, x, op):
+        import torch
+
+        if self.world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        torch.distributed.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        import torch
+
+        return self._reduce(x, torch.distributed.ReduceOp.MAX if self.world > 1 else None)
+
+    def sum(self, x):
+        import torch
+
+        return self._reduce(x, torch.distributed.ReduceOp.SUM if self.world > 1 else None)
 
 
 def sssp_bytes(nv, e_reached):
@@ -269,28 +311,12 @@ def run_ours(a):
 
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
 
-    def barrier():
-        if dist:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks(world, torch.device("cuda", local))
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
     ctx = sg.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    h, srcs = make_graph(a.scale)
+    h, srcs = make_graph(a.scale, rank)
     nv, ne = h.nv, h.ne
     G = ctx.graph(h)
     dout = torch.empty(nv, dtype=torch.int32, device="cuda")
