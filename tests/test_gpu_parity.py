@@ -259,3 +259,28 @@ def test_device_checked_upload_matches_host_path(ctx):
         a, _, _ = Gd.sssp(s, priority="low_high", max_iteration=1000000)
         b, _, _ = Gh.sssp(s, priority="low_high", max_iteration=1000000)
         assert (a == b).all() and (a == oracle.sssp(h.offsets, h.indices, h.weights, s)).all()
+
+
+def test_device_wait_timeout_reports_status_and_context_recovers(ctx):
+    """Failure detection without a fault: a star's hub expanded by one thread
+    (push load balancing off) holds every other block at the round barrier far
+    longer than a 1 ns bound, so their bounded waits give up, the launch
+    returns SG_ERR_TIMEOUT (a leader that gives up releases the others with an
+    abort bit), and the same context then runs a normal query exactly."""
+    n = 1 << 20
+    off = np.full(n + 2, n, np.uint32)
+    off[0] = 0
+    idx = np.arange(1, n + 1, dtype=np.uint32)
+    G = ctx.graph_from_csr(off, idx, no_csc=True)
+    seen = None
+    for _ in range(3):
+        try:
+            G.bfs(0, variant="async_push_dd", lb_push="none", timeout_s=1e-9)
+        except sg.SGError as e:
+            seen = e.status
+            break
+    assert seen == 4, seen  # SG_ERR_TIMEOUT
+    lv, st, _ = G.bfs(0, variant="async_push_dd", lb_push="none")
+    assert st.device_error == 0
+    assert lv[0] == 0 and (lv[1:] == 1).all()
+    G.close()
