@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <vector>
 
 #include "sg_runtime.cuh"
@@ -46,23 +47,24 @@ __device__ __forceinline__ K key_max() {
     return (K)~(K)0;
 }
 
-// Temporary device buffers of one build call; freed after the stream drains.
+// Temporary device buffers of one call, named in the context's grow-only
+// scratch (released by sg_ctx_release_cached): repeated builds and
+// transposes reuse them instead of allocating and freeing every time.  Each
+// call site has its own prefix and each allocation of a Tmp its own number,
+// so buffers whose lifetimes overlap never share a name; a later call with
+// the same prefix reuses the buffers of an earlier one, which is finished by
+// then (all work of a context is ordered on its stream).
 struct Tmp {
     sg_ctx *ctx;
-    std::vector<void *> ptrs;
-    explicit Tmp(sg_ctx *c) : ctx(c) {}
-    ~Tmp() {
-        if (!ptrs.empty()) cudaStreamSynchronize(ctx->stream);
-        for (void *p : ptrs) cudaFree(p);
-    }
+    const char *prefix;
+    unsigned n = 0;
+    Tmp(sg_ctx *c, const char *p) : ctx(c), prefix(p) {}
     template <class T>
     cudaError_t alloc(T **p, uint64_t count) {
-        void *q = nullptr;
-        cudaError_t e = cudaMalloc(&q, std::max<uint64_t>(count, 1) * sizeof(T));
-        if (e != cudaSuccess) return e;
-        ptrs.push_back(q);
-        *p = (T *)q;
-        return cudaSuccess;
+        char name[48];
+        std::snprintf(name, sizeof name, "gb_%s_%u", prefix, n++);
+        if (!ctx->graph_ws) ctx->graph_ws = new Workspace;
+        return ctx->graph_ws->get(name, (size_t)std::max<uint64_t>(count, 1), p);
     }
 };
 
@@ -370,7 +372,7 @@ template <class K>
 sg_status sort_rows(sg_ctx *ctx, const uint32_t *off, uint32_t nv, uint64_t n, K *keys) {
     if (n < 2) return SG_OK;
     const cudaStream_t s = ctx->stream;
-    Tmp tmp(ctx);
+    Tmp tmp(ctx, "sort");
     const uint32_t wrows_cap = (uint32_t)(n / 33 + 1), mid_cap = (uint32_t)(n / (kWarpKeys + 1) + 1);
     const uint32_t big_cap = (uint32_t)(n / (kSmemKeys + 1) + 1);
     uint2 *wrows, *mid, *big;
@@ -691,7 +693,7 @@ sg_status device_transpose(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32_t
                            const uint32_t *w, uint32_t *crow, uint32_t *ccol, uint32_t *cw) {
     using namespace gbuild;
     const cudaStream_t s = ctx->stream;
-    Tmp tmp(ctx);
+    Tmp tmp(ctx, "tr");
     uint32_t *cnt;
     SG_TRY_CUDA(ctx, tmp.alloc(&cnt, (uint64_t)nv + 1));
     SG_TRY_CUDA(ctx, cudaMemsetAsync(cnt, 0, 4ull * (nv + 1), s));
@@ -717,7 +719,7 @@ sg_status device_compare_csr(sg_ctx *ctx, uint32_t nv, uint64_t ne, const uint32
                              bool *structure_differs, bool *weights_differ) {
     using namespace gbuild;
     const cudaStream_t s = ctx->stream;
-    Tmp tmp(ctx);
+    Tmp tmp(ctx, "cmp");
     uint32_t *diff, hd[2];
     SG_TRY_CUDA(ctx, tmp.alloc(&diff, 2));
     SG_TRY_CUDA(ctx, cudaMemsetAsync(diff, 0, 8, s));
@@ -739,7 +741,7 @@ sg_status symmetric_weighted_csc(sg_ctx *ctx, sg_graph *g) {
     using namespace gbuild;
     const uint32_t nv = g->nv;
     const uint64_t ne = g->ne;
-    Tmp tmp(ctx);
+    Tmp tmp(ctx, "sym");
     uint32_t *trow, *tcol, *tw;
     SG_TRY_CUDA(ctx, tmp.alloc(&trow, (uint64_t)nv + 1));
     SG_TRY_CUDA(ctx, tmp.alloc(&tcol, ne));
@@ -810,7 +812,7 @@ sg_status sg_graph_build(sg_ctx *ctx, uint32_t nv, uint64_t m, const uint32_t *s
     if (m > kMaxEntries) return set_error(ctx, SG_ERR_INVALID_ARG, "%llu edges exceed the uint32 entry range", (unsigned long long)m);
     if (d2ud) graph_flags |= SG_GRAPH_SYMMETRIC;
     const cudaStream_t s = ctx->stream;
-    Tmp tmp(ctx);
+    Tmp tmp(ctx, "in");
 
     // inputs on the device
     EdgeList el{src, dst, weights, m, nv, 0u, (build_flags & SG_BUILD_DESELF_CYCLE) != 0};
