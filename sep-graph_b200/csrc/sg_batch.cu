@@ -431,7 +431,7 @@ sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint3
 
     static int bps = 0;
     if (!bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, msbfs_kernel, kMsThreads, 0));
-    const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : 4;
+    const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::ms_blocks_per_sm(nv, g->ne);
     dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(bps, want)));
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));

@@ -198,6 +198,18 @@ struct EngineResult {
     uint32_t device_error() const { return ctrl.error | ctrl.cnt.error; }
 };
 
+// Resident blocks per SM of the multi-source kernels (BFS masks, BC lanes)
+// when the caller does not choose: sparse high-diameter graphs are bound by
+// the per-level barrier (fewer blocks), large dense ones by memory latency
+// (more).  Measured on B200: 16 BFS on the 4096^2 grid 197 / 229 / 288 ms with
+// 2 / 4 / 6 blocks; 64 BFS and 32 BC on symmetric RMAT-22 9.4 -> 8.2 and
+// 23.3 -> 21.1 ms from 4 to 6; RMAT-16 best with 4.
+inline int ms_blocks_per_sm(uint32_t nv, uint64_t ne) {
+    const double avg_deg = nv ? (double)ne / nv : 0.0;
+    if (avg_deg < 8) return 2;
+    return ne >= (1ull << 25) ? 6 : 4;
+}
+
 // Resident blocks per SM when the caller does not choose: small graphs are
 // bound by per-round barrier latency, which grows with the number of blocks.
 inline int auto_blocks_per_sm(uint32_t nv, uint64_t ne) {
