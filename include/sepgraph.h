@@ -99,7 +99,9 @@ typedef struct sg_options {
     int32_t local_depth;      /* levels a block follows its own discoveries before a round ends
                                  (0 = off; with variant SG_ASYNC_PUSH_DD and functors whose
                                  ReorderSafe() holds only) */
-    int32_t reserved[2];
+    int32_t wl_sort;          /* --wl_sort: sort the worklist of each data-driven push round by vertex id
+                                 (framework.cuh:488-496); single-query calls, batches ignore it */
+    int32_t reserved[1];
 } sg_options;
 
 /* Per-round trace record (the reference's --trace line, framework.cuh:334-348). */

@@ -247,6 +247,7 @@ inline sg_options CommonOptions() {
     o.lb_push = parse_lb(FLAGS_lb_push);
     o.lb_pull = parse_lb(FLAGS_lb_pull);
     o.trace = FLAGS_trace;
+    o.wl_sort = FLAGS_wl_sort;
     o.blocks_per_sm = FLAGS_grid_size > 0 && FLAGS_grid_size <= 32 ? FLAGS_grid_size : 0;
     return o;
 }

@@ -149,6 +149,9 @@ struct KArgs {
     sg_round_trace *trace;
     uint32_t trace_cap;
     Params p;
+    // --wl_sort scratch: nwords bitmap words (zero between sorts), then one
+    // count per block of the team; null = worklists are not sorted
+    uint32_t *sort_bits = nullptr;
 };
 
 // Leader-only policy state (RunningInfo), lives in block 0 / thread 0.
@@ -653,6 +656,82 @@ struct EngineKernel {
             const uint32_t v = dev::ld_l2(Q + i);
             dev::bitmap_clear(a.qflag[s.qin], v);
             if (to_bitmap) dev::bitmap_set(a.bitmap[s.bin], v);  // Queue2Bitmap (driver.cuh:119-129)
+        }
+    }
+
+    // ---------------------------------------------------------------- --wl_sort
+    // The reference sorts the worklist of every data-driven push round by
+    // vertex id (thrust::sort, framework.cuh:488-496).  Worklists here hold no
+    // duplicates, so the sort is a bitmap pass in three barrier-separated
+    // phases: every item sets its vertex's bit; each block counts the bits of
+    // its contiguous word range; each block writes its range's vertices in
+    // ascending order at the sum of the counts before it (clearing the words,
+    // so the bitmap is zero for the next sort).
+
+    // Block-wide exclusive scan of x; *total = the block's sum.  All threads call.
+    static __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *total) {
+        __shared__ uint32_t part[kWarpsPerBlock];
+        const uint32_t lane = dev::lane_id(), wid = threadIdx.x >> 5;
+        const uint32_t incl = dev::warp_inclusive_scan(x);
+        if (lane == 31) part[wid] = incl;
+        __syncthreads();
+        uint32_t before = 0, sum = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kWarpsPerBlock; ++k) {
+            const uint32_t p = part[k];
+            if (k < wid) before += p;
+            sum += p;
+        }
+        __syncthreads();  // part[] is free for the next call
+        *total = sum;
+        return before + incl - x;
+    }
+
+    static __device__ __forceinline__ void sort_range(const Args &a, uint32_t &w0, uint32_t &w1) {
+        const uint32_t per = (a.nwords + g_team_size - 1) / g_team_size;
+        w0 = min(a.nwords, g_team_rank * per);
+        w1 = min(a.nwords, w0 + per);
+    }
+
+    static __device__ void sort_mark(const Args &a, const Snap &s) {
+        const uint32_t *Q = a.queue[s.qin];
+        for (uint32_t i = gthread(); i < s.F; i += nthreads()) {
+            const uint32_t v = dev::ld_l2(Q + i);
+            atomicOr(a.sort_bits + (v >> 5), 1u << (v & 31u));
+        }
+    }
+
+    static __device__ void sort_count(const Args &a) {
+        uint32_t w0, w1, total;
+        sort_range(a, w0, w1);
+        uint32_t cnt = 0;
+        for (uint32_t w = w0 + threadIdx.x; w < w1; w += blockDim.x) cnt += __popc(dev::ld_l2(a.sort_bits + w));
+        block_exclusive_scan(cnt, &total);
+        if (threadIdx.x == 0) __stcg(a.sort_bits + a.nwords + g_team_rank, total);
+    }
+
+    static __device__ void sort_emit(const Args &a, const Snap &s) {
+        uint32_t w0, w1, total;
+        sort_range(a, w0, w1);
+        uint32_t before = 0;
+        for (uint32_t b = threadIdx.x; b < g_team_rank; b += blockDim.x) before += dev::ld_l2(a.sort_bits + a.nwords + b);
+        block_exclusive_scan(before, &total);
+        uint32_t off = total;
+        uint32_t *Q = a.queue[s.qin];
+        for (uint32_t base = w0; base < w1; base += blockDim.x) {  // block-uniform trip count
+            const uint32_t w = base + threadIdx.x;
+            uint32_t x = 0;
+            if (w < w1) {
+                x = dev::ld_l2(a.sort_bits + w);
+                if (x) __stcg(a.sort_bits + w, 0u);
+            }
+            const uint32_t c = __popc(x);
+            uint32_t pos = off + block_exclusive_scan(c, &total);
+            while (x) {
+                __stcg(Q + pos++, w * 32u + (uint32_t)(__ffs(x) - 1));
+                x &= x - 1;
+            }
+            off += total;
         }
     }
 
@@ -1333,6 +1412,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         a.qflag[0][w] = 0;
         a.qflag[1][w] = 0;
         a.qflag[2][w] = 0;
+        if (a.sort_bits) a.sort_bits[w] = 0;
     }
     if (!grid_sync(c, tmo, nop)) return false;
     K::rebuild(app, a, 0, acc);
@@ -1349,6 +1429,14 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         K::set_app_variant(app, var);
         app.m_concurrent_combine =
             var == V_ASYNC_PUSH_DD && a.p.local_depth > 0 && a.p.forced == V_ASYNC_PUSH_DD && reorder_safe(app);
+        if (var == V_ASYNC_PUSH_DD && a.sort_bits && s.F > 1) {  // --wl_sort
+            K::sort_mark(a, s);
+            if (!grid_sync(c, tmo, nop)) return false;
+            K::sort_count(a);
+            if (!grid_sync(c, tmo, nop)) return false;
+            K::sort_emit(a, s);
+            if (!grid_sync(c, tmo, nop)) return false;
+        }
         if (s.chunks) {
             // chunks of the heavy vertices the previous push round found (reorder-safe functors only)
             K::heavy_phase(app, a, s, set ^ 1u, true, acc);

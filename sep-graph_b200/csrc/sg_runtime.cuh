@@ -186,6 +186,7 @@ struct EngineConfig {
     uint32_t chunk_edges = 256;
     uint32_t local_depth = 0;  // local lookahead levels in push rounds (0 = off)
     float sample_cut = 0.f;    // sampling priority cut in ASYNC_PUSH_TD rounds (0 = off)
+    bool wl_sort = false;      // sort each data-driven push round's worklist by vertex id (--wl_sort)
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -328,6 +329,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     bps = std::max(1, std::min(bps, max_blocks_per_sm));
     dim3 grid(ctx->prop.multiProcessorCount * bps), block(kBlockThreads);
     res->grid_blocks = grid.x;
+    if (cfg.wl_sort) SG_TRY_CUDA(ctx, ws.get("sort", (uint64_t)nwords + grid.x, &a.sort_bits));
 
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));

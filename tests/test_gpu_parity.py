@@ -174,6 +174,53 @@ def test_bc_rmat(ctx):
         assert np.allclose(bc, bc64, rtol=BC_RTOL, atol=BC_ATOL)
 
 
+@pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
+def test_wl_sort_golden(ctx, path):
+    """--wl_sort on the small fixtures (fewer bitmap words than blocks: most
+    blocks own an empty range of the sort)."""
+    g = _load(path)
+    G = _graph(ctx, g)
+    src = int(g["source"])
+    for kw in (dict(), dict(variant="async_push_dd"), dict(variant="async_push_dd", lb_push="none")):
+        lv, _, _ = G.bfs(src, wl_sort=1, **kw)
+        assert (lv == g["bfs"]).all(), kw
+    for kw in (dict(variant="async_push_dd"), dict(priority="low_high")):
+        d, _, _ = G.sssp(src, wl_sort=1, max_iteration=100000, **kw)
+        assert (d == g["sssp"]).all(), kw
+
+
+@pytest.mark.parametrize("bps", [1, 8])
+def test_wl_sort_same_results(ctx, bps):
+    """--wl_sort (framework.cuh:488-496): every data-driven push round takes its
+    worklist in ascending vertex order.  Results equal the oracle's, and a
+    level-synchronous BFS takes the same rounds as without the sort."""
+    h = sg.HostGraph.rmat(15, 16, symmetric=True, seed=1).gen_weights(1, 64, 2)
+    G = ctx.graph(h, symmetric=True)
+    src = int(h.max_degree_vertex()[0])
+    ref = oracle.bfs(h.offsets, h.indices, src)
+    for kw in (dict(), dict(variant="async_push_dd"), dict(variant="async_push_dd", lb_push="none"),
+               dict(variant="async_push_dd", local_depth=16)):
+        lv0, st0, _ = G.bfs(src, blocks_per_sm=bps, **kw)
+        lv, st, _ = G.bfs(src, blocks_per_sm=bps, wl_sort=1, **kw)
+        assert (lv == ref).all() and (lv0 == ref).all(), kw
+        if "local_depth" not in kw:
+            assert st.rounds == st0.rounds, (kw, st.rounds, st0.rounds)
+    ref = oracle.sssp(h.offsets, h.indices, h.weights, src)
+    for kw in (dict(variant="async_push_dd"), dict(priority="low_high"),
+               dict(priority="low_high", priority_delta=8, variant="async_push_dd", local_depth=16)):
+        d, _, _ = G.sssp(src, blocks_per_sm=bps, wl_sort=1, max_iteration=100000, **kw)
+        assert (d == ref).all(), kw
+    bc, sigma, _ = G.bc(src, blocks_per_sm=bps, wl_sort=1, variant="async_push_dd")
+    bc64, sig64, _ = oracle.bc_f64(h.offsets, h.indices, src)
+    assert (sigma.astype(np.float64) == sig64).all()
+    assert np.allclose(bc, bc64, rtol=BC_RTOL, atol=BC_ATOL)
+    hp = sg.HostGraph.rmat(14, 16, symmetric=False, seed=1)
+    Gp = ctx.graph(hp)
+    r, _, _ = Gp.pagerank(variant="async_push_dd", wl_sort=1, blocks_per_sm=bps, pr_error=1e-7,
+                          max_iteration=100000)
+    assert _pr_l1(r, oracle.pagerank_f64(hp.offsets, hp.indices, 1e-12)) <= PR_L1_TOL
+
+
 # ---------------------------------------------------------------- engine behaviour
 def test_policy_switches_direction_and_trace(ctx):
     h = sg.HostGraph.rmat(16, 16, symmetric=True, seed=1)

@@ -279,3 +279,36 @@ def test_market_reader_matches_reference(tmp_path, weighted):
     assert np.array_equal(src, rs) and np.array_equal(h.indices, rd)
     if weighted:
         assert np.array_equal(h.weights, rw)
+
+
+def test_ctypes_mirrors_match_c_header_layout(tmp_path):
+    """Every ctypes structure of the binding has the size and field offsets
+    that a C compiler gives the matching struct of include/sepgraph.h."""
+    import shutil
+    import ctypes as C
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    pairs = {"sg_options": sg.Options, "sg_round_trace": sg.RoundTrace, "sg_stats": sg.Stats,
+             "sg_batch_query": sg.BatchQuery, "sg_server_config": sg.ServerConfig, "sg_query": sg.Query,
+             "sg_server_stats": sg.ServerStats, "sg_tune_entry": sg.TuneEntry}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "sepgraph.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    r = subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=30).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
+    assert sg.make_options().wl_sort == 0
