@@ -149,9 +149,8 @@ struct KArgs {
     sg_round_trace *trace;
     uint32_t trace_cap;
     Params p;
-    // --wl_sort scratch: nwords bitmap words (zero between sorts), then one
-    // count per block of the team; null = worklists are not sorted
-    uint32_t *sort_bits = nullptr;
+    // --wl_sort: one count per block of the team; null = worklists are not sorted
+    uint32_t *sort_counts = nullptr;
 };
 
 // Leader-only policy state (RunningInfo), lives in block 0 / thread 0.
@@ -661,12 +660,13 @@ struct EngineKernel {
 
     // ---------------------------------------------------------------- --wl_sort
     // The reference sorts the worklist of every data-driven push round by
-    // vertex id (thrust::sort, framework.cuh:488-496).  Worklists here hold no
-    // duplicates, so the sort is a bitmap pass in three barrier-separated
-    // phases: every item sets its vertex's bit; each block counts the bits of
-    // its contiguous word range; each block writes its range's vertices in
-    // ascending order at the sum of the counts before it (clearing the words,
-    // so the bitmap is zero for the next sort).
+    // vertex id (thrust::sort, framework.cuh:488-496).  Here the input slot's
+    // queued bitmap already holds exactly the worklist's vertices when a round
+    // starts (every bit set comes with an append to that slot, and bits are
+    // cleared only while the slot is the input), so the sort is a pass over
+    // that bitmap in two barrier-separated phases: each block counts the bits
+    // of its contiguous word range; each block writes its range's vertices in
+    // ascending order at the sum of the counts before it.
 
     // Block-wide exclusive scan of x; *total = the block's sum.  All threads call.
     static __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *total) {
@@ -693,38 +693,28 @@ struct EngineKernel {
         w1 = min(a.nwords, w0 + per);
     }
 
-    static __device__ void sort_mark(const Args &a, const Snap &s) {
-        const uint32_t *Q = a.queue[s.qin];
-        for (uint32_t i = gthread(); i < s.F; i += nthreads()) {
-            const uint32_t v = dev::ld_l2(Q + i);
-            atomicOr(a.sort_bits + (v >> 5), 1u << (v & 31u));
-        }
-    }
-
-    static __device__ void sort_count(const Args &a) {
+    static __device__ void sort_count(const Args &a, const Snap &s) {
         uint32_t w0, w1, total;
         sort_range(a, w0, w1);
+        const uint32_t *bits = a.qflag[s.qin];
         uint32_t cnt = 0;
-        for (uint32_t w = w0 + threadIdx.x; w < w1; w += blockDim.x) cnt += __popc(dev::ld_l2(a.sort_bits + w));
+        for (uint32_t w = w0 + threadIdx.x; w < w1; w += blockDim.x) cnt += __popc(dev::ld_l2(bits + w));
         block_exclusive_scan(cnt, &total);
-        if (threadIdx.x == 0) __stcg(a.sort_bits + a.nwords + g_team_rank, total);
+        if (threadIdx.x == 0) __stcg(a.sort_counts + g_team_rank, total);
     }
 
     static __device__ void sort_emit(const Args &a, const Snap &s) {
         uint32_t w0, w1, total;
         sort_range(a, w0, w1);
         uint32_t before = 0;
-        for (uint32_t b = threadIdx.x; b < g_team_rank; b += blockDim.x) before += dev::ld_l2(a.sort_bits + a.nwords + b);
+        for (uint32_t b = threadIdx.x; b < g_team_rank; b += blockDim.x) before += dev::ld_l2(a.sort_counts + b);
         block_exclusive_scan(before, &total);
         uint32_t off = total;
+        const uint32_t *bits = a.qflag[s.qin];
         uint32_t *Q = a.queue[s.qin];
         for (uint32_t base = w0; base < w1; base += blockDim.x) {  // block-uniform trip count
             const uint32_t w = base + threadIdx.x;
-            uint32_t x = 0;
-            if (w < w1) {
-                x = dev::ld_l2(a.sort_bits + w);
-                if (x) __stcg(a.sort_bits + w, 0u);
-            }
+            uint32_t x = w < w1 ? dev::ld_l2(bits + w) : 0u;
             const uint32_t c = __popc(x);
             uint32_t pos = off + block_exclusive_scan(c, &total);
             while (x) {
@@ -1412,7 +1402,6 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         a.qflag[0][w] = 0;
         a.qflag[1][w] = 0;
         a.qflag[2][w] = 0;
-        if (a.sort_bits) a.sort_bits[w] = 0;
     }
     if (!grid_sync(c, tmo, nop)) return false;
     K::rebuild(app, a, 0, acc);
@@ -1429,10 +1418,8 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         K::set_app_variant(app, var);
         app.m_concurrent_combine =
             var == V_ASYNC_PUSH_DD && a.p.local_depth > 0 && a.p.forced == V_ASYNC_PUSH_DD && reorder_safe(app);
-        if (var == V_ASYNC_PUSH_DD && a.sort_bits && s.F > 1) {  // --wl_sort
-            K::sort_mark(a, s);
-            if (!grid_sync(c, tmo, nop)) return false;
-            K::sort_count(a);
+        if (var == V_ASYNC_PUSH_DD && a.sort_counts && s.F > 1) {  // --wl_sort
+            K::sort_count(a, s);
             if (!grid_sync(c, tmo, nop)) return false;
             K::sort_emit(a, s);
             if (!grid_sync(c, tmo, nop)) return false;

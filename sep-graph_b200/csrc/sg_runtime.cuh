@@ -329,7 +329,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     bps = std::max(1, std::min(bps, max_blocks_per_sm));
     dim3 grid(ctx->prop.multiProcessorCount * bps), block(kBlockThreads);
     res->grid_blocks = grid.x;
-    if (cfg.wl_sort) SG_TRY_CUDA(ctx, ws.get("sort", (uint64_t)nwords + grid.x, &a.sort_bits));
+    if (cfg.wl_sort) SG_TRY_CUDA(ctx, ws.get("sort", grid.x, &a.sort_counts));
 
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
