@@ -333,22 +333,29 @@ __global__ void __launch_bounds__(kMbThreads) msbc_kernel(MbArgs a) {
         if (!engine::grid_sync(c, a.timeout_ns, close_level)) return;
     }
     if (ovf) atomicOr(&n->error, dev::kErrOverflow);
+    // A level list that ran out of room is incomplete and its level ends point
+    // past the entries written: the host retries with the full bound, so this
+    // launch stops here.  Every block reads the same bit (nothing sets it
+    // after the forward pass's last barrier) and returns before the backward
+    // pass's first barrier.
+    if (dev::ld_l2(&n->error) & dev::kErrCapacity) return;
 
     // ---------------------------------------------------------------- backward
     // levels 0 .. L-1 hold entries (the last appended level was empty); the
-    // deepest level has delta 0, so q = 1 / sigma there
+    // deepest level has delta 0, so q = 1 / sigma there.  Level ends are
+    // clamped to the list's capacity as a second guard.
+    auto end_of = [&](uint32_t d) { return min(dev::ld_l2(a.ends + d), a.list_cap); };
     const uint32_t L = dev::ld_l2(&c->round) - 1;
     const uint32_t nch1 = min(dev::ld_l2(a.counts + 2), a.chunk_cap);
     if (L >= 2) {
-        const uint32_t b0 = dev::ld_l2(a.ends + L - 1), e0 = dev::ld_l2(a.ends + L);
+        const uint32_t b0 = end_of(L - 1), e0 = end_of(L);
         for (uint32_t i = b0 + gw; i < e0; i += nw) {
             const uint2 en = a.list[i];
             if ((en.y >> lane) & 1u) finish_dep(a, en.x, 0.f);
         }
     }
     for (int d = (int)L - 2; d >= 1; --d) {
-        const uint32_t b0 = dev::ld_l2(a.ends + d), e0 = dev::ld_l2(a.ends + d + 1);
-        const uint32_t e1 = dev::ld_l2(a.ends + d + 2);
+        const uint32_t b0 = end_of(d), e0 = end_of(d + 1), e1 = end_of(d + 2);
         // masks of level d+1 and level d, dense
         for (uint32_t i = b0 + gthread(); i < e1; i += nthreads()) {
             const uint2 en = a.list[i];
