@@ -227,6 +227,22 @@ def test_msbc_split_hubs(ctx):
     _msbc_case(ctx, h, srcs, False)
 
 
+def test_msbc_level_list_retry_long_chain(ctx):
+    """A two-way chain of 2000 vertices with 32 sources spread along it: each
+    vertex sits at up to 32 distinct depths, so the first launch's level list
+    (8 entries per vertex) overflows and the call is retried with the bound
+    of 32; the overflowed launch stops before its backward pass and the rows
+    still equal the oracle's."""
+    n = 2000
+    off, idx = [0], []
+    for v in range(n):
+        idx += [u for u in (v - 1, v + 1) if 0 <= u < n]
+        off.append(len(idx))
+    h = sg.HostGraph.from_csr(np.array(off, np.uint32), np.array(idx, np.uint32))
+    srcs = [int(x) for x in np.linspace(0, n - 1, 32).round()]
+    _msbc_case(ctx, h, srcs, True)
+
+
 def test_msbc_rejects_bad_input(ctx):
     h = sg.HostGraph.rmat(8, 8, seed=1)
     G = ctx.graph(h)
