@@ -63,7 +63,8 @@ static bool HybridBC() {
     st.trace_capacity = (uint32_t)trace.size();
     JsonRecord js;
     SG_CHECK(sg_bc(g.dev, src, &o, bc.data(), sigma.data(), &st));
-    PrintRun(st, o, js);
+    PrintRun(st, o, g, false, js);
+    js.put("time_stage2", st.time_total_ms - st.time_kernel_ms);  // hybrid_bc.cu:296-300
     bool ok = true;
     if (FLAGS_check) {
         std::vector<double> rb, rs;

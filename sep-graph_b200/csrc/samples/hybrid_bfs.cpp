@@ -37,7 +37,7 @@ static bool HybridBFS() {
     st.trace_capacity = (uint32_t)trace.size();
     JsonRecord js;
     SG_CHECK(sg_bfs(g.dev, src, &o, levels.data(), &st));
-    PrintRun(st, o, js);
+    PrintRun(st, o, g, false, js);
     js.put("non_atomic", FLAGS_non_atomic ? "YES" : "NO");
     bool ok = true;
     if (FLAGS_check) {

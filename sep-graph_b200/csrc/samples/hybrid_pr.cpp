@@ -68,7 +68,7 @@ static bool HybridPageRank() {
     st.trace_capacity = (uint32_t)trace.size();
     JsonRecord js;
     SG_CHECK(sg_pagerank(g.dev, &o, ranks.data(), residual.data(), &st));
-    PrintRun(st, o, js);
+    PrintRun(st, o, g, true, js);
     js.put("error_tolerance", FLAGS_error);
     double sum = 0;
     for (float r : ranks) sum += r;

@@ -37,7 +37,7 @@ static bool HybridSSSP() {
     st.trace_capacity = (uint32_t)trace.size();
     JsonRecord js;
     SG_CHECK(sg_sssp(g.dev, src, &o, dist.data(), &st));
-    PrintRun(st, o, js);
+    PrintRun(st, o, g, false, js);
     bool ok = true;
     if (FLAGS_check) {
         const auto ref = HostSSSP(g, src);

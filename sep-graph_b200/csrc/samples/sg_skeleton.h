@@ -73,20 +73,56 @@ DEFINE_int32(device, 0, "CUDA device");
 
 static sg_ctx *g_ctx = nullptr;
 
-// Minimal JSON record written when --json is set (JsonWriter, src/utils/to_json.cpp:8-61).
+// The run record written when --json is set (JsonWriter, src/utils/to_json.cpp:8-61):
+// one object with the keys of Engine::SaveToJson (framework.cuh:205-257) and the
+// sample's own, numbers, strings and string lists, keys sorted and indented by
+// four spaces as the reference's writer prints them.
 struct JsonRecord {
-    std::vector<std::pair<std::string, std::string>> kv;
+    std::map<std::string, std::string> kv;  // key -> serialised value
+    static std::string quote(const std::string &s) {
+        std::string r = "\"";
+        for (unsigned char ch : s) {
+            if (ch == '"' || ch == '\\') {
+                r += '\\';
+                r += (char)ch;
+            } else if (ch < 0x20) {
+                char b[8];
+                std::snprintf(b, sizeof b, "\\u%04x", ch);
+                r += b;
+            } else {
+                r += (char)ch;
+            }
+        }
+        return r + "\"";
+    }
     void put(const std::string &k, double v) {
         char b[64];
-        std::snprintf(b, sizeof b, "%.9g", v);
-        kv.emplace_back(k, b);
+        if (std::isfinite(v)) std::snprintf(b, sizeof b, "%.9g", v);
+        else std::snprintf(b, sizeof b, "null");
+        kv[k] = b;
     }
-    void put(const std::string &k, const std::string &v) { kv.emplace_back(k, "\"" + v + "\""); }
+    void put_int(const std::string &k, long long v) { kv[k] = std::to_string(v); }
+    void put(const std::string &k, const std::string &v) { kv[k] = quote(v); }
+    void put(const std::string &k, const char *v) { kv[k] = quote(v); }
+    void put(const std::string &k, const std::vector<std::string> &v) {
+        if (v.empty()) {
+            kv[k] = "[]";
+            return;
+        }
+        std::string r = "[\n";
+        for (size_t i = 0; i < v.size(); ++i) r += "        " + quote(v[i]) + (i + 1 < v.size() ? ",\n" : "\n");
+        kv[k] = r + "    ]";
+    }
+    double get(const std::string &k) const {
+        auto it = kv.find(k);
+        return it == kv.end() ? 0.0 : std::atof(it->second.c_str());
+    }
     ~JsonRecord() {
         if (FLAGS_json.empty()) return;
         std::ofstream f(FLAGS_json);
-        f << "{";
-        for (size_t i = 0; i < kv.size(); ++i) f << (i ? ", " : "") << "\"" << kv[i].first << "\": " << kv[i].second;
+        f << "{\n";
+        size_t i = 0;
+        for (const auto &e : kv) f << "    " << quote(e.first) << ": " << e.second << (++i < kv.size() ? ",\n" : "\n");
         f << "}\n";
     }
 };
@@ -252,16 +288,33 @@ inline sg_options CommonOptions() {
     return o;
 }
 
-// PrintInfo / --trace lines (framework.cuh:259-313, 334-348).
-inline void PrintRun(const sg_stats &st, const sg_options &o, JsonRecord &js) {
+inline const char *lb_name(int lb) {  // LBToString (common.h:179-200)
+    switch (lb) {
+        case SG_LB_NONE: return "NONE";
+        case SG_LB_COARSE_GRAINED: return "COARSED_GRAINED";
+        case SG_LB_FINE_GRAINED: return "FINE_GRAINED";
+        case SG_LB_HYBRID: return "HYBRID";
+        default: return "UNKNOWN";
+    }
+}
+
+// PrintInfo / --trace lines (framework.cuh:259-313, 334-348) and the run
+// record's SaveToJson keys (framework.cuh:205-257).  `iterative` is the
+// engine's AlgoType (ITERATIVE_SCHEME for PageRank).
+inline void PrintRun(const sg_stats &st, const sg_options &o, const LoadedGraph &g, bool iterative, JsonRecord &js) {
+    std::vector<std::string> rounds;
     if (FLAGS_trace)
         for (uint32_t i = 0; i < st.n_trace; ++i) {
             const sg_round_trace &t = st.trace[i];
-            std::printf(
-                "Round: %u Policy to execute: %s Time: %f In-nodes: %u Out-nodes: %u Input-edges: %llu Output-edges: "
-                "%llu Total-workload: %lld\n",
-                t.round, variant_name(t.variant), t.time_ms, t.in_nodes, t.out_nodes,
-                (unsigned long long)t.in_workload, (unsigned long long)t.out_workload, (long long)t.total_workload);
+            char line[512];
+            std::snprintf(line, sizeof line,
+                          "Round: %u Policy to execute: %s Time: %f In-nodes: %u Out-nodes: %u Input-edges: %llu "
+                          "Output-edges: %llu Total-workload: %lld",
+                          t.round, variant_name(t.variant), t.time_ms, t.in_nodes, t.out_nodes,
+                          (unsigned long long)t.in_workload, (unsigned long long)t.out_workload,
+                          (long long)t.total_workload);
+            std::printf("%s\n", line);
+            rounds.emplace_back(line);
         }
     std::printf("--------------Time statistics---------\n");
     std::printf("Kernel time: %f\n", st.time_kernel_ms);
@@ -275,13 +328,37 @@ inline void PrintRun(const sg_stats &st, const sg_options &o, JsonRecord &js) {
     std::printf("Max iteration reached: %s\n", st.max_iteration_reached ? "YES" : "NO");
     std::printf("Edges reached: %llu  GTEPS: %f\n", (unsigned long long)st.edges_reached,
                 st.time_total_ms > 0 ? st.edges_reached / st.time_total_ms / 1e6 : 0.0);
+    // The reference times these host-side stages around separate kernels; here
+    // they run inside the one device-resident launch and are part of time_kernel.
+    for (const char *k : {"time_input_active_node", "time_output_active_node", "time_input_workload",
+                          "time_output_workload", "time_queue2bitmap", "time_bitmap2queue", "time_rebuild_worklist",
+                          "time_priority_sample", "time_sort_worklist", "time_unique_worklist"})
+        js.put(k, 0.0);
     js.put("time_kernel", st.time_kernel_ms);
     js.put("time_total", st.time_total_ms);
     js.put("time_per_round", st.rounds ? st.time_total_ms / st.rounds : 0.0);
-    js.put("num_iteration", (double)st.rounds);
-    js.put("max_iteration_reached", st.max_iteration_reached ? "YES" : "NO");
-    js.put("dataset", FLAGS_graphfile);
+    js.put_int("num_iteration", st.rounds);
     if (o.variant >= 0) js.put("force_variant", variant_name(o.variant));
+    if (o.lb_push != SG_LB_AUTO) js.put("force_push_load_balancing", lb_name(o.lb_push));
+    if (o.lb_pull != SG_LB_AUTO) js.put("force_pull_load_balancing", lb_name(o.lb_pull));
+    if (o.priority == SG_PRIORITY_LOW_HIGH) {
+        js.put("priority_type", "low_high");
+        js.put("priority_delta", o.priority_delta);
+    } else if (o.priority == SG_PRIORITY_SAMPLING) {
+        js.put("priority_type", "sampling");
+        js.put("cut_threshold", o.cut_threshold);
+    } else {
+        js.put("priority_type", "none");
+    }
+    js.put("fused_kernel", o.fused ? "YES" : "NO");
+    js.put("max_iteration_reached", st.max_iteration_reached ? "YES" : "NO");
+    char dev[256] = "";
+    if (g_ctx && sg_device_info(g_ctx, nullptr, nullptr, nullptr, dev, sizeof dev) == SG_OK) js.put("device", dev);
+    js.put("dataset", FLAGS_graphfile);
+    js.put_int("nnodes", g.nv);
+    js.put_int("nedges", (long long)g.ne);
+    js.put("algo_type", iterative ? "ITERATIVE_SCHEME" : "TRAVERSAL_SCHEME");
+    if (FLAGS_trace) js.put("round", rounds);
 }
 
 // ---- host checkers behind --check (FIFO BFS / label-correcting SSSP /

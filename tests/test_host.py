@@ -312,3 +312,63 @@ def test_ctypes_mirrors_match_c_header_layout(tmp_path):
         for f in py._fields_:
             assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
     assert sg.make_options().wl_sort == 0
+
+
+def test_sample_run_record_format(tmp_path):
+    """The samples' --json record: every key of the reference's
+    Engine::SaveToJson (framework.cuh:205-257) with its value type, the trace
+    lines under "round", keys sorted, strings escaped (built on the CPU from
+    synthetic statistics through the samples' own PrintRun)."""
+    import json
+    import shutil
+
+    cxx = shutil.which("g++")
+    lib = os.path.join(ROOT, "sep-graph_b200", "libsepgraph_b200.so")
+    if not cxx or not os.path.exists(lib):
+        pytest.skip("no C++ compiler or library not built")
+    out = tmp_path / "rec.json"
+    src = tmp_path / "rec.cpp"
+    src.write_text(r'''
+#include "sg_skeleton.h"
+int main(int argc, char **argv) {
+    sgflags::ParseCommandLineFlags(&argc, &argv, true);
+    sg_round_trace tr[2] = {{1, SG_ASYNC_PUSH_DD, 1, 5, 3, 40, 100, 0.5f, 0}, {2, SG_ASYNC_PULL_DD, 5, 0, 0, 0, 60, 0.25f, 0}};
+    sg_stats st{};
+    st.rounds = 2; st.time_total_ms = 1.5; st.time_kernel_ms = 1.25; st.trace = tr; st.n_trace = 2; st.trace_capacity = 2;
+    sg_options o; sg_options_default(&o);
+    o.variant = SG_ASYNC_PUSH_DD; o.lb_push = SG_LB_FINE_GRAINED; o.priority = SG_PRIORITY_LOW_HIGH; o.priority_delta = 8;
+    LoadedGraph g; g.nv = 10; g.ne = 30;
+    JsonRecord js;
+    PrintRun(st, o, g, false, js);
+    js.put("non_atomic", "YES");
+    return 0;
+}
+''')
+    exe = tmp_path / "rec"
+    inc = os.path.join(ROOT, "sep-graph_b200", "csrc", "samples")
+    r = subprocess.run([cxx, "-std=c++17", "-O0", "-I", inc, str(src), "-o", str(exe), "-L",
+                        os.path.dirname(lib), "-lsepgraph_b200", "-Wl,-rpath," + os.path.dirname(lib)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-3000:]
+    r = subprocess.run([str(exe), "--trace", f"--json={out}", '--graphfile=a "quoted"\\path.gr'],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    text = out.read_text()
+    rec = json.loads(text)
+    save_to_json = {"time_input_active_node", "time_output_active_node", "time_input_workload",
+                    "time_output_workload", "time_queue2bitmap", "time_bitmap2queue", "time_rebuild_worklist",
+                    "time_priority_sample", "time_sort_worklist", "time_unique_worklist", "time_kernel", "time_total",
+                    "time_per_round", "num_iteration", "force_variant", "force_push_load_balancing",
+                    "priority_type", "priority_delta", "fused_kernel", "max_iteration_reached", "dataset", "nnodes",
+                    "nedges", "algo_type", "round"}
+    assert save_to_json <= set(rec), save_to_json - set(rec)
+    assert "force_pull_load_balancing" not in rec and "device" not in rec  # not forced; no context
+    assert rec["num_iteration"] == 2 and rec["nnodes"] == 10 and rec["nedges"] == 30
+    assert rec["time_total"] == 1.5 and rec["time_per_round"] == 0.75 and rec["time_kernel"] == 1.25
+    assert rec["force_variant"] == "ASYNC_PUSH_DD" and rec["force_push_load_balancing"] == "FINE_GRAINED"
+    assert rec["priority_type"] == "low_high" and rec["priority_delta"] == 8
+    assert rec["algo_type"] == "TRAVERSAL_SCHEME" and rec["fused_kernel"] == "NO" and rec["non_atomic"] == "YES"
+    assert rec["dataset"] == 'a "quoted"\\path.gr'
+    assert rec["round"] == [l for l in r.stdout.splitlines() if l.startswith("Round: ")]
+    assert len(rec["round"]) == 2 and "ASYNC_PULL_DD" in rec["round"][1]
+    assert list(rec) == sorted(rec) and text.startswith("{\n    \"")
