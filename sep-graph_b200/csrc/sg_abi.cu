@@ -662,8 +662,9 @@ sg_status sg_bc(sg_graph *g, uint32_t source, const sg_options *opt, float *bc_o
         ba.bar = misc + 4;
         ba.err = misc + 3;
         ba.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
-        static int bps = 0;
-        if (!bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, bc_backward_kernel, 256, 0));
+        static std::atomic<int> occupancy{0};
+        int bps = 0;
+        SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, (const void *)bc_backward_kernel, 256, &bps));
         dim3 grid(ctx->prop.multiProcessorCount * std::max(1, bps));
         void *args[] = {&ba};
         SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));

@@ -429,8 +429,9 @@ sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint3
     a.force_dir = o.variant == SG_ASYNC_PUSH_DD ? 0 : (o.variant == SG_ASYNC_PULL_DD ? 1 : -1);
     if (!g->has_csc && !g->symmetric) a.force_dir = 0;
 
-    static int bps = 0;
-    if (!bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, msbfs_kernel, kMsThreads, 0));
+    static std::atomic<int> occupancy{0};
+    int bps = 0;
+    SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, (const void *)msbfs_kernel, kMsThreads, &bps));
     const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::ms_blocks_per_sm(nv, g->ne);
     dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(bps, want)));
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
@@ -673,8 +674,9 @@ sg_status prepare_batch(sg_ctx *ctx, sgb::Workspace &ws, std::vector<engine::Bat
     B.bc = kBC;
     B.value_bytes = sizeof(TV);
     B.kernel = kBC ? (const void *)batched_bc_kernel : (const void *)batched_engine_kernel<App, TV, TB, TW>;
-    static int max_bps = 0;
-    if (!max_bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_bps, B.kernel, kBlockThreads, 0));
+    static std::atomic<int> occupancy{0};  // one per template instantiation
+    int max_bps = 0;
+    SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, B.kernel, kBlockThreads, &max_bps));
     const int bps = std::max(1, std::min(max_bps, o.blocks_per_sm > 0 ? o.blocks_per_sm : 4));
     const uint32_t total_blocks = (uint32_t)(ctx->prop.multiProcessorCount * bps);
     // Automatic team size.  Equal teams claim queries largest first, so the

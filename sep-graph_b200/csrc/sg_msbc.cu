@@ -460,8 +460,9 @@ sg_status msbc_rows(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const s
     else SG_TRY_CUDA(ctx, ws.get("mb_bc", (size_t)nsrc * nv, &a.bc));
     a.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);
 
-    static int bps = 0;
-    if (!bps) SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, msbc_kernel, kMbThreads, 0));
+    static std::atomic<int> occupancy{0};
+    int bps = 0;
+    SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, (const void *)msbc_kernel, kMbThreads, &bps));
     if (bps <= 0) return sgb::set_error(ctx, SG_ERR_NO_DEVICE, "multi-source BC kernel cannot be resident");
     const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::ms_blocks_per_sm(nv, g->ne);
     const dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(bps, want)));

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -199,6 +200,20 @@ struct EngineResult {
     uint32_t device_error() const { return ctrl.error | ctrl.cnt.error; }
 };
 
+// Resident blocks per SM of `kernel` at `threads` threads per block, computed
+// on first use and cached in `cache` (one per kernel, shared by the server's
+// worker threads).
+inline cudaError_t occupancy_once(std::atomic<int> &cache, const void *kernel, int threads, int *out) {
+    int v = cache.load(std::memory_order_relaxed);
+    if (v == 0) {
+        const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, 0);
+        if (e != cudaSuccess) return e;
+        cache.store(v, std::memory_order_relaxed);
+    }
+    *out = v;
+    return cudaSuccess;
+}
+
 // Resident blocks per SM of the multi-source kernels (BFS masks, BC lanes)
 // when the caller does not choose: sparse high-diameter graphs are bound by
 // the per-level barrier (fewer blocks), large dense ones by memory latency
@@ -320,11 +335,10 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     app.m_p_current_round = &a.ctrl->rs.round;
 
     auto kernel = hybrid_engine_kernel<App, TV, TB, TW>;
-    static int max_blocks_per_sm = 0;  // one per template instantiation
-    if (max_blocks_per_sm == 0) {
-        SG_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks_per_sm, kernel, kBlockThreads, 0));
-        if (max_blocks_per_sm <= 0) return set_error(ctx, SG_ERR_NO_DEVICE, "engine kernel cannot be resident");
-    }
+    static std::atomic<int> occupancy{0};  // one per template instantiation
+    int max_blocks_per_sm = 0;
+    SG_TRY_CUDA(ctx, occupancy_once(occupancy, (const void *)kernel, kBlockThreads, &max_blocks_per_sm));
+    if (max_blocks_per_sm <= 0) return set_error(ctx, SG_ERR_NO_DEVICE, "engine kernel cannot be resident");
     int bps = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : auto_blocks_per_sm(nv, ne);
     bps = std::max(1, std::min(bps, max_blocks_per_sm));
     dim3 grid(ctx->prop.multiProcessorCount * bps), block(kBlockThreads);
