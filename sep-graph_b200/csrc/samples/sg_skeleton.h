@@ -442,7 +442,7 @@ struct Skeleton {
     }
 
     // Returns 0 when the run (and --check) passed; the reference prints the
-    // verdict but always returns 0 (app_skeleton.h:155-156).
+    // check's outcome but always returns 0 (app_skeleton.h:155-156).
     int Run() {
         std::printf("\nTesting single GPU %s\n--------------------\n\n", App::NameUpper());
         const bool ok = App::Single();
