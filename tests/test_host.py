@@ -341,6 +341,7 @@ int main(int argc, char **argv) {
     JsonRecord js;
     PrintRun(st, o, g, false, js);
     js.put("non_atomic", "YES");
+    std::printf("wl_sort=%d\n", CommonOptions().wl_sort);
     return 0;
 }
 ''')
@@ -350,7 +351,7 @@ int main(int argc, char **argv) {
                         os.path.dirname(lib), "-lsepgraph_b200", "-Wl,-rpath," + os.path.dirname(lib)],
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr[-3000:]
-    r = subprocess.run([str(exe), "--trace", f"--json={out}", '--graphfile=a "quoted"\\path.gr'],
+    r = subprocess.run([str(exe), "--trace", "--wl_sort", f"--json={out}", '--graphfile=a "quoted"\\path.gr'],
                        capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stderr
     text = out.read_text()
@@ -372,3 +373,4 @@ int main(int argc, char **argv) {
     assert rec["round"] == [l for l in r.stdout.splitlines() if l.startswith("Round: ")]
     assert len(rec["round"]) == 2 and "ASYNC_PULL_DD" in rec["round"][1]
     assert list(rec) == sorted(rec) and text.startswith("{\n    \"")
+    assert "wl_sort=1" in r.stdout  # --wl_sort reaches sg_options
