@@ -95,3 +95,24 @@ def test_reference_arm_runs_on_rank0_only(monkeypatch):
     t0 = __import__("time").perf_counter()
     assert bench.run_reference(types.SimpleNamespace(scale=22, steps=1, warmup=1)) is None
     assert __import__("time").perf_counter() - t0 < 1.0  # returned without building the graph
+
+
+def test_reference_arm_line_on_rank0(monkeypatch, capsys):
+    """The reference arm on rank 0 times the reference's CPU SSSP on a small
+    graph and prints one JSON line with the fields the driver reads."""
+    import json
+
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "sep-graph_b200")]
+    import bench
+
+    monkeypatch.setenv("RANK", "0")
+    bench.run_reference(types.SimpleNamespace(scale=12, steps=1, warmup=0, gpus=1))
+    lines = [l for l in capsys.readouterr().out.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    rec = json.loads(lines[0])
+    assert rec["impl"] == "reference" and rec["metric"] == rec["unit"] == bench.METRIC and rec["value"] > 0
+    assert rec["steps"] == 1 and rec["n_gpus"] == 1 and rec["higher_is_better"] is True
+    assert rec["cpu_baseline"]["kind"] in ("reference", "port") and rec["cpu_baseline"]["cores"] >= 1
+    assert rec["cpu_baseline"]["value"] == rec["value"]
+    assert rec["e2e"] == {"value": rec["value"], "unit": rec["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert rec["config"]["workload"] == bench.WORKLOAD and rec["config"]["nv"] == 4096
