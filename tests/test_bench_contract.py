@@ -5,7 +5,7 @@ import os
 import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-sys.path[:0] = [ROOT]
+sys.path[:0] = [ROOT, os.path.join(ROOT, "sep-graph_b200")]
 
 import bench  # noqa: E402
 
@@ -40,3 +40,38 @@ def test_clock_summary_skips_unreadable_values_and_lines():
 def test_clock_summary_without_samples():
     assert _clocks("")["reasons"] == ["unsampled"]
     assert _clocks(None)["sm_mhz"] is None
+
+
+def test_algorithmic_bytes_and_roofline_arithmetic():
+    # SSSP: offsets + (index + weight) per reached edge + distances; BFS: index only
+    assert bench.sssp_bytes(10, 100) == 4 * 11 + 8 * 100 + 4 * 10
+    assert bench.bfs_bytes(10, 100) == 4 * 11 + 4 * 100 + 4 * 10
+    r = bench._roof(2e9, 1.0, 4000.0)  # 2 GB in 1 ms = 2000 GB/s
+    assert abs(r["GBs"] - 2000.0) < 1e-9 and abs(r["frac_hbm"] - 0.5) < 1e-12
+    assert abs(r["frac_hbm_nominal_8TBs"] - 0.25) < 1e-12
+
+
+def test_reached_edges_counts_out_degrees_of_reached_vertices():
+    import numpy as np
+    import types
+
+    h = types.SimpleNamespace(offsets=np.array([0, 2, 3, 3, 6], np.uint32))
+    vals = np.array([0, 1, bench.INF, 2], np.uint32)
+    assert bench.reached_edges(h, vals) == 2 + 1 + 3
+
+
+def test_traffic_comes_from_the_committed_summaries():
+    for mode in ("delta8", "push"):
+        t = bench.read_traffic(mode)
+        assert t is not None and t > 0, mode
+    peak, kind = bench.peak_hbm()
+    assert peak > 0 and kind in ("measured", "fallback")
+
+
+def test_cpu_baseline_record():
+    import sepgraph as sg
+
+    h = sg.HostGraph.rmat(10, 8, seed=1).gen_weights(1, 64, 2)
+    srcs = [int(s) for s in h.pick_sources(3, 3)]
+    b = bench.cpu_baseline(h, srcs, budget_s=5.0)
+    assert b["value"] > 0 and b["cores"] == 1 and b["kind"] in ("reference", "port") and b["unit"] == bench.METRIC
