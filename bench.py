@@ -180,6 +180,23 @@ def make_graph(scale, rank=0):
     return h, replica_sources(h, rank)
 
 
+def make_graph_reference(scale):
+    """The same graph and rank-0 sources from the oracle's generator (a CPU test
+    proves its CSR, weights and sources equal to the library's, word for word),
+    so the reference arm never loads the library."""
+    import oracle
+
+    h = oracle.rmat(scale, EDGE_FACTOR, 0.57, 0.19, 0.19, seed=1).gen_weights(1, 64, 2)
+    return h, replica_sources(h, 0)
+
+
+def config_of(nv, ne, n_sources, world):
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "nv": nv, "ne": ne, "sources_per_step": n_sources,
+            "l2": "inputs larger than L2 (graph arrays %.0f MB vs 126 MB L2)" % ((4 * (nv + 1) + 8 * ne) / 1e6),
+            "parallelism": f"replicas{world}"}
+
+
 def replica_sources(h, rank):
     return [int(s) for s in h.pick_sources(N_SOURCES, 3 if rank == 0 else 3 + 1000 * rank)]
 
@@ -245,34 +262,37 @@ def cpu_sssp_one(h, src):
 
 
 def cpu_baseline(h, srcs, budget_s=20.0):
-    """Single thread, as many sources as fit the budget (>= 1)."""
+    """Single thread, as many sources as fit the budget (>= 1); also returns each
+    computed distance array under "results" (the caller checks the GPU's against them)."""
     t_tot, e_tot, n = 0.0, 0, 0
     kind = "port"
+    results = {}
     for s in srcs:
         t0 = time.perf_counter()
         d, kind = cpu_sssp_one(h, s)
         t_tot += time.perf_counter() - t0
         e_tot += reached_edges(h, d)
+        results[s] = d
         n += 1
         if t_tot > budget_s:
             break
     return {"value": e_tot / t_tot / 1e9, "unit": METRIC, "cores": 1, "kind": kind,
             "sample": f"SSSPHostNaive from {n} of the {len(srcs)} sources on the full RMAT-{SCALE} graph, 1 thread",
-            "seconds": t_tot}
+            "seconds": t_tot, "results": results}
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    h, srcs = make_graph(a.scale)
+    h, srcs = make_graph_reference(a.scale)
     ncores = os.cpu_count() or 1
     nthreads = min(ncores, len(srcs))
 
     def step():
         t0 = time.perf_counter()
         with cf.ThreadPoolExecutor(nthreads) as ex:  # ctypes releases the GIL during the C call
-            outs = list(ex.map(lambda s: cpu_sssp_one(h, s), srcs[:nthreads]))
+            outs = list(ex.map(lambda s: cpu_sssp_one(h, s), srcs))
         dt = time.perf_counter() - t0
         e = sum(reached_edges(h, d) for d, _ in outs)
         return e, dt, outs[0][1]
@@ -288,9 +308,10 @@ def run_reference(a):
     line = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * tot_t / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nv": h.nv, "ne": h.ne, "sources_per_step": nthreads},
+            "config": config_of(h.nv, h.ne, len(srcs), a.gpus),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": nthreads, "kind": kind,
-                             "sample": f"{nthreads} sources per step, one thread each, full graph"},
+                             "sample": f"all {len(srcs)} sources of the step on {nthreads} threads (one source "
+                                       "per thread at a time), full graph"},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -331,10 +352,11 @@ def run_ours(a):
     best = "{variant}{d}".format(variant=tuned["variant"], d=f"_delta{tuned['priority_delta']:g}"
                                  if "priority" in tuned else "")
     mode_ms = [dict(r) for r in report]
-    e_reached = {}
+    e_reached, gpu_dist = {}, {}
     for s in srcs:
-        _, st, _ = G.sssp(s, **kw)
+        d, st, _ = G.sssp(s, **kw)
         e_reached[s] = st.edges_reached
+        gpu_dist[s] = d
     step_edges = sum(e_reached[s] for s in srcs)
     step_bytes = sum(sssp_bytes(nv, e_reached[s]) for s in srcs)
     kw_async = dict(kw, blocking=0)
@@ -397,9 +419,19 @@ def run_ours(a):
     h2d = 4 * (nv + 1) + 8 * ne
     d2h = 4 * nv * len(srcs)
 
-    cpu = None
+    # ---- parity at the headline configuration: every source's distances
+    # against the oracle's Dijkstra (exact: distances are unique), and against
+    # the reference's own SSSPHostNaive for the sources the CPU baseline runs
+    parity_fail = 0
+    for s in srcs:
+        parity_fail += int(not np.array_equal(gpu_dist[s], oracle_dijkstra(h, s)))
+    cpu, ref_checked = None, 0
     if rank == 0 and world == 1:
         cpu = cpu_baseline(h, srcs)
+        for s, d in cpu.pop("results").items():
+            parity_fail += int(not np.array_equal(gpu_dist[s], d))
+            ref_checked += 1
+    parity_fail = int(sum_over_ranks(parity_fail))
     peak, peak_kind = peak_hbm()
     avg_launch_ms = float(np.mean(launch_ms))
     achieved = (step_bytes / len(srcs)) / (avg_launch_ms * 1e-3) / 1e9
@@ -408,11 +440,13 @@ def run_ours(a):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "nv": nv, "ne": ne, "sources_per_step": len(srcs), "mode": best,
-                   "options": tuned, "autotune_ms_per_source": tuned_ms, "autotune_report": mode_ms,
-                   "edges_reached_per_step": step_edges,
-                   "l2": "inputs larger than L2 (graph arrays %.0f MB vs 126 MB L2)" % ((4 * (nv + 1) + 8 * ne) / 1e6),
-                   "parallelism": f"replicas{world}"},
+        "config": config_of(nv, ne, len(srcs), world),
+        "tuning": {"mode": best, "options": tuned, "autotune_ms_per_source": tuned_ms, "autotune_report": mode_ms,
+                   "edges_reached_per_step": step_edges},
+        "parity": {"sssp_rmat22_headline": parity_fail == 0,
+                   "checked": f"{len(srcs) * world} sources' distances vs the oracle's Dijkstra (all ranks); "
+                              f"{ref_checked} of them also vs the reference's SSSPHostNaive (rank 0), bit-exact",
+                   "mismatched_sources": parity_fail},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "what": "per step: pinned CSR+weights upload and device check into the graph arena the context kept from the previous step (sg_graph_destroy keeps it for reuse), 8 queries into pinned host distance arrays, graph released",
                 "ms_per_step": {k: 1e3 * v / e2e_steps for k, v in parts.items()}},
@@ -442,12 +476,37 @@ def run_ours(a):
         for k, (_, g) in list(cache.items()):
             if k != "rmat22":
                 g.close()
+    if "extra" in line:
+        for name, sec in line["extra"].items():
+            for k, v in _parity_flags(sec, name):
+                line["parity"][k] = v
     if rank == 0:
         print(json.dumps(line), flush=True)
     G.close()
     ctx.close()
     if dist:
         torch.distributed.destroy_process_group()
+    if parity_fail:
+        sys.exit(3)  # a fast wrong answer is not a result
+
+
+def _parity_flags(sec, prefix):
+    """(name, bool) for every parity boolean an extra section reports."""
+    out = []
+    if not isinstance(sec, dict):
+        return out
+    for k, v in sec.items():
+        if isinstance(v, dict):
+            out += _parity_flags(v, f"{prefix}.{k}")
+        elif isinstance(v, bool) and ("parity" in k or "same" in k or "agree" in k or k.endswith("_ok")):
+            out.append((f"{prefix}.{k}", v))
+    return out
+
+
+def oracle_dijkstra(h, s):
+    import oracle
+
+    return oracle.dijkstra(h.offsets, h.indices, h.weights, s)
 
 
 def read_traffic(mode):
@@ -515,11 +574,16 @@ def per_algo(ctx, cache, a):
     src = 0
     tuned, _, report = G.autotune("sssp", [src], max_iteration=10000000)
     t, (d, st, _) = _median_ms(lambda: G.sssp(src, max_iteration=10000000, **tuned), 6)
+    t0 = time.perf_counter()
+    ok = bool(np.array_equal(d, oracle.dijkstra(h.offsets, h.indices, h.weights, src)))
+    dij_s = time.perf_counter() - t0
     res["sssp_grid4096_w1-1000"] = dict(
         GTEPS=st.edges_reached / t / 1e6, ms=t, rounds=st.rounds, options=tuned,
         autotune_report=report, candidates_agree=not any(r["status"] == 10 for r in report),
+        parity_vs_oracle=ok, parity_how="distances bit-exact vs the oracle's Dijkstra (unique shortest distances)",
         us_per_round=1e3 * t / max(1, st.rounds), **_roof(sssp_bytes(h.nv, st.edges_reached), t, peak),
-        cpu="not timed: the reference's SSSPHostNaive needs about 4 minutes on one core for this graph")
+        cpu="the reference's SSSPHostNaive needs about 4 minutes on one core for this graph (not timed); "
+            f"the oracle's binary-heap Dijkstra took {dij_s:.1f} s on one core")
     G.close()
     del h, d
 
@@ -540,6 +604,16 @@ def per_algo(ctx, cache, a):
         ranks[v] = np.asarray(r, np.float64)
     p0, p1 = ranks["async_push_dd"], ranks["sync_pull_td"]
     pr["l1_push_vs_pull_normalised"] = float(np.abs(p0 / p0.sum() - p1 / p1.sum()).sum())
+    # FP64 oracle: PageRankHost's fixed point by parallel Jacobi sweeps to a 1e-13 relative L1 change
+    t0 = time.perf_counter()
+    ref64, sweeps = oracle.pagerank_fixed_point_f64(h.offsets, h.indices, 1e-13)
+    pr["oracle"] = {"sweeps": sweeps, "seconds": time.perf_counter() - t0, "threads": oracle.host_threads(),
+                    "what": "FP64 fixed point of PageRankHost, Jacobi sweeps to a 1e-13 relative L1 change"}
+    for v in ("async_push_dd", "sync_pull_td"):
+        l1 = float(np.abs(ranks[v] / ranks[v].sum() - ref64 / ref64.sum()).sum())
+        pr[v]["l1_vs_fp64_oracle"] = l1
+        pr[v]["parity_vs_oracle"] = l1 <= 1e-6
+    del ref64
     G.close()
     del h, ranks
     # CPU: PageRankHost at the same threshold on a bounded sample (RMAT-20, same generator)
@@ -563,14 +637,25 @@ def per_algo(ctx, cache, a):
     b = 2 * (4 * (h.nv + 1) + 4 * e_r) + 32 * h.nv
     cpu_s = _cpu_time(lambda: oracle.ref_bc(h.offsets, h.indices, src) if ref else oracle.bc_f32(h.offsets, h.indices, src),
                       budget_s=40.0)
+    bc64, sig64, _ = oracle.bc_f64(h.offsets, h.indices, src)
+    err = np.abs(bc.astype(np.float64) - bc64)
+    ok_bc = bool(np.all(err <= 1e-4 * np.abs(bc64) + 1e-5))
+    ok_sig = bool(np.array_equal(np.asarray(sig, np.float64), sig64))
     res["bc_rmat23_sym"] = dict(GTEPS=2 * e_r / t / 1e6, ms=t, rounds=st.rounds, **_roof(b, t, peak),
+                                parity_vs_oracle=ok_bc and ok_sig,
+                                parity_how="BC within 1e-4 relative + 1e-5 of the FP64 oracle, path counts exact",
+                                max_rel_err_where_above_1=float(np.max((err / np.abs(bc64))[np.abs(bc64) > 1])
+                                                                if np.any(np.abs(bc64) > 1) else 0.0),
                                 cpu_GTEPS=2 * e_r / cpu_s / 1e9, cpu_ms=1e3 * cpu_s, cpu=cpu_kind)
+    del bc64, sig64
     G.close()
     return res
 
 
 def batched(ctx, cache, a):
-    """Batched launches against one plain launch per query, same results required."""
+    """Batched launches against one plain launch per query, same results required;
+    a sample of the plain results is checked against the oracle."""
+    import oracle
     import sepgraph as sg
 
     res = {}
@@ -582,6 +667,7 @@ def batched(ctx, cache, a):
         lv, st, _ = G.bfs(s)
         plain_ms += st.time_kernel_ms
         plain.append(lv)
+    plain_ok = all(np.array_equal(plain[i], oracle.bfs(h.offsets, h.indices, srcs[i])) for i in range(4))
     ms_t, (outs, st_t, _) = _median_ms(lambda: ctx.bfs_batch([(G, s) for s in srcs]), 3)
     same_t = all((o == p).all() for o, p in zip(outs, plain))
     ms_m, (lv_m, st_m) = _median_ms(lambda: G.msbfs(srcs), 3)
@@ -591,7 +677,8 @@ def batched(ctx, cache, a):
         "plain_ms": plain_ms, "plain_qps": 64 / (plain_ms * 1e-3), "plain_GTEPS": e / plain_ms / 1e6,
         "team_batch_ms": ms_t, "team_batch_qps": 64 / (ms_t * 1e-3), "team_batch_GTEPS": e / ms_t / 1e6,
         "team_blocks": st_t.vertices_reached, "teams": st_t.search_depth, "team_batch_same_results": same_t,
-        "msbfs_ms": ms_m, "msbfs_qps": 64 / (ms_m * 1e-3), "msbfs_GTEPS": e / ms_m / 1e6, "msbfs_same_results": same_m}
+        "msbfs_ms": ms_m, "msbfs_qps": 64 / (ms_m * 1e-3), "msbfs_GTEPS": e / ms_m / 1e6, "msbfs_same_results": same_m,
+        "plain_parity_vs_oracle_first4": plain_ok}
     del plain, outs, lv_m
 
     # the same on a high-diameter graph: 16 sources on the 4096x4096 grid
@@ -616,6 +703,11 @@ def batched(ctx, cache, a):
         bc, _, st = G.bc(s)
         plain_ms += st.time_total_ms
         plain.append(bc)
+    bc_ok = True
+    for i in range(2):
+        bc64, _, _ = oracle.bc_f64(h.offsets, h.indices, srcs32[i])
+        bc_ok &= bool(np.all(np.abs(plain[i] - bc64) <= 1e-4 * np.abs(bc64) + 1e-5))
+    del bc64
     ms_b, (outs, st_b, _) = _median_ms(lambda: ctx.bc_batch([(G, s) for s in srcs32]), 3)
     same_b = all(np.allclose(o, p, rtol=1e-4, atol=1e-5) for o, p in zip(outs, plain))
     ms_mb, (rows_mb, _) = _median_ms(lambda: G.msbc(srcs32), 3)
@@ -624,7 +716,7 @@ def batched(ctx, cache, a):
                               "batch_qps": 32 / (ms_b * 1e-3), "same_results_rtol_1e-4": same_b,
                               "batch_GTEPS": st_b.edges_reached / ms_b / 1e6,
                               "msbc_ms": ms_mb, "msbc_qps": 32 / (ms_mb * 1e-3),
-                              "msbc_same_results_rtol_1e-4": same_mb}
+                              "msbc_same_results_rtol_1e-4": same_mb, "plain_parity_vs_oracle_first2": bc_ok}
     G.close()
     del h, plain, outs
 
@@ -644,6 +736,10 @@ def batched(ctx, cache, a):
         d, st, _ = gg.sssp(s, **kw)
         plain_ms += st.time_kernel_ms
         plain.append(d)
+    sssp_ok = all(np.array_equal(plain[k], oracle.dijkstra(graphs[k % len(graphs)][0].offsets,
+                                                         graphs[k % len(graphs)][0].indices,
+                                                         graphs[k % len(graphs)][0].weights, queries[k][1]))
+                  for k in range(0, 256, 16))
     ms_s, (outs, st_s, _) = _median_ms(lambda: ctx.sssp_batch(queries, **kw), 3)
     same_s = all((o == p).all() for o, p in zip(outs, plain))
     # the same batch planned once and replayed as a CUDA graph into device outputs
@@ -665,7 +761,7 @@ def batched(ctx, cache, a):
                                 "batch_GTEPS": st_s.edges_reached / ms_s / 1e6, "teams": st_s.search_depth,
                                 "team_blocks": st_s.vertices_reached, "plan_ms": ms_p,
                                 "plan_qps": 256 / (ms_p * 1e-3), "plan_cuda_graph": captured,
-                                "plan_same_results": same_p}
+                                "plan_same_results": same_p, "plain_parity_vs_oracle_every16th": sssp_ok}
     for _, gg in graphs:
         gg.close()
     return res

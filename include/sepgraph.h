@@ -355,7 +355,11 @@ sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources, uint32_t n
  * graph, NULL for push-only) and levels_out are device memory of the current
  * device.  The first call on a device looks up the array's address; make it
  * before any stream capture.  Calls share the array: calls that overlap on the
- * GPU race.  Blocks until done; err (optional) receives a message. */
+ * GPU race.  opt NULL = sg_options_default(); automatic choices (load
+ * balancing, blocks per SM) follow sg_bfs's rules.  stats (optional) gets
+ * rounds, max_iteration_reached, rounds_by_variant, edges_processed,
+ * vertices_processed and device_error; its time and reached-vertex fields and
+ * n_trace are set to 0.  Blocks until done; err (optional) receives a message. */
 sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *indices, uint32_t nv, uint64_t ne,
                          const uint32_t *in_offsets, const uint32_t *in_indices, uint32_t source,
                          const sg_options *opt, uint32_t *levels_out, void *cuda_stream, sg_stats *stats, char *err,

@@ -44,6 +44,13 @@ def lib() -> C.CDLL:
         L.sgo_pagerank_f64.argtypes = [C.c_uint32, _P, _P, C.c_double, _P, _P]
         L.sgo_bc_f32.argtypes = [C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P]
         L.sgo_bc_f64.argtypes = [C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P]
+        L.sgo_rmat_edges.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int,
+                                     _P, _P]
+        L.sgo_build_csr.argtypes = [C.c_uint32, C.c_uint64, _P, _P, C.c_int, C.c_int, _P, _P, C.POINTER(C.c_uint64)]
+        L.sgo_gen_weights.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _P]
+        L.sgo_pick_sources.argtypes = [C.c_uint32, _P, C.c_uint32, C.c_uint64, _P]
+        L.sgo_dijkstra.argtypes = [C.c_uint32, _P, _P, _P, C.c_uint32, _P]
+        L.sgo_pagerank_jacobi_f64.argtypes = [C.c_uint32, _P, _P, C.c_double, C.c_uint32, _P, C.POINTER(C.c_uint32)]
         _o = L
     return _o
 
@@ -119,6 +126,82 @@ def bc_f64(offsets, indices, src):
     bc, sg, lv = np.empty(n, np.float64), np.empty(n, np.float64), np.empty(n, np.uint32)
     assert lib().sgo_bc_f64(n, _p(o), _p(i), src, _p(bc), _p(sg), _p(lv)) == 0
     return bc, sg, lv
+
+
+# ---------------------------------------------------------------- full-size inputs and checkers
+class Graph:
+    """A CSR graph made by the oracle's generators (numpy arrays)."""
+
+    def __init__(self, offsets, indices, weights=None):
+        self.offsets, self.indices, self.weights = offsets, indices, weights
+        self.nv, self.ne = len(offsets) - 1, len(indices)
+
+    def max_degree_vertex(self):
+        """GetMaxOutDgrNode (include/groute/graphs/csr_graph.h:241-259): lowest id among the maximum out-degree."""
+        d = np.diff(self.offsets.astype(np.int64))
+        v = int(np.argmax(d))
+        return v, int(d[v])
+
+    def pick_sources(self, n, seed):
+        out = np.empty(n, np.uint32)
+        assert lib().sgo_pick_sources(self.nv, _p(self.offsets), n, seed, _p(out)) == 0
+        return out
+
+    def gen_weights(self, lo, hi, seed):
+        w = np.empty(self.ne, np.uint32)
+        assert lib().sgo_gen_weights(self.ne, lo, hi, seed, _p(w)) == 0
+        self.weights = w
+        return self
+
+
+def rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, symmetric=False, keep_self_loops=False,
+         keep_duplicates=False) -> Graph:
+    """The seeded RMAT graph (the same CSR as the product library's generator, word for word)."""
+    m = edge_factor << scale
+    tot = 2 * m if symmetric else m
+    src, dst = np.empty(tot, np.uint32), np.empty(tot, np.uint32)
+    assert lib().sgo_rmat_edges(scale, edge_factor, a, b, c, seed, int(symmetric), _p(src), _p(dst)) == 0
+    off = np.empty((1 << scale) + 1, np.uint32)
+    ne = C.c_uint64()
+    assert lib().sgo_build_csr(1 << scale, tot, _p(src), _p(dst), int(keep_self_loops), int(keep_duplicates),
+                               _p(off), _p(dst_buf := np.empty(tot, np.uint32)), C.byref(ne)) == 0
+    del src, dst
+    return Graph(off, dst_buf[: ne.value].copy())
+
+
+def grid(rows, cols) -> Graph:
+    """4-neighbour grid, both directions, each row's neighbours in increasing id order."""
+    nv = rows * cols
+    v = np.arange(nv, dtype=np.int64)
+    r, c = v // cols, v % cols
+    nb = np.stack([np.where(r > 0, v - cols, -1), np.where(c > 0, v - 1, -1),
+                   np.where(c + 1 < cols, v + 1, -1), np.where(r + 1 < rows, v + cols, -1)], axis=1)
+    ok = nb >= 0
+    off = np.zeros(nv + 1, np.uint32)
+    off[1:] = np.cumsum(ok.sum(axis=1))
+    return Graph(off, nb[ok].astype(np.uint32))
+
+
+def dijkstra(offsets, indices, weights, src):
+    """Shortest-path distances (unique for uint32 weights: what SSSPHostNaive returns)."""
+    o, i = _u32(offsets), _u32(indices)
+    w = _u32(weights) if weights is not None else None
+    out = np.empty(len(o) - 1, np.uint32)
+    assert lib().sgo_dijkstra(len(o) - 1, _p(o), _p(i), _p(w), src, _p(out)) == 0
+    return out
+
+
+def pagerank_fixed_point_f64(offsets, indices, tol=1e-13, max_iter=2000):
+    """PageRankHost's fixed point in double, by parallel Jacobi sweeps; returns (ranks, sweeps)."""
+    o, i = _u32(offsets), _u32(indices)
+    out = np.empty(len(o) - 1, np.float64)
+    it = C.c_uint32()
+    assert lib().sgo_pagerank_jacobi_f64(len(o) - 1, _p(o), _p(i), tol, max_iter, _p(out), C.byref(it)) == 0
+    return out, it.value
+
+
+def host_threads() -> int:
+    return int(lib().sgo_threads())
 
 
 # ---------------------------------------------------------------- graph construction

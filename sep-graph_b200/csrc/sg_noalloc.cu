@@ -19,6 +19,15 @@
 // call's contents, so calls whose work overlaps on the GPU (different streams,
 // or different host threads on one device) race and must be serialised by the
 // caller.
+//
+// Options: opt == NULL means sg_options_default(), and every automatic choice
+// (load balancing from the average degree, resident blocks per SM from the
+// graph's size) is made as sg_bfs makes it, so both run the same rounds.
+// Statistics filled: rounds, max_iteration_reached, rounds_by_variant,
+// edges_processed, vertices_processed and device_error.  The call creates no
+// timing events, so time_total_ms and time_kernel_ms are set to 0, as are the
+// reached-vertex fields (edges_reached, vertices_reached, search_depth) and
+// n_trace (no trace is recorded).
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -27,6 +36,7 @@
 
 #include "sg_apps.cuh"
 #include "sg_engine.cuh"
+#include "sg_runtime.cuh"
 
 namespace {
 
@@ -120,24 +130,16 @@ extern "C" sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *ind
         }
         base = g_scratch_addr[dev];
     }
+    cudaStream_t s = (cudaStream_t)stream;
     sg_options o;
-    if (opt) {
+    if (opt)
         o = *opt;
-    } else {
-        std::memset(&o, 0, sizeof o);
-        o.variant = SG_VARIANT_AUTO;
-        o.alpha = 15;
-        o.beta = 18;
-        o.edge_factor = 1.0;
-        o.max_iteration = 200;
-        o.non_atomic = 1;
-        o.timeout_s = 30;
-    }
+    else
+        sg_options_default(&o);
     const bool has_csc = in_offsets != nullptr;
     if (!has_csc && o.variant >= 0 && (o.variant >> 1) & 1)
         return fail(err, err_len, SG_ERR_UNSUPPORTED, "sg_bfs_noalloc: pull variants need the in-edge arrays");
 
-    cudaStream_t s = (cudaStream_t)stream;
     engine::KArgs<uint32_t, uint32_t, graphs::NoWeight> a;
     std::memset(&a, 0, sizeof a);
     a.csr.nnodes = nv;
@@ -199,7 +201,7 @@ extern "C" sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *ind
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, engine::kBlockThreads, 0);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) {
-        const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : 2;
+        const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::auto_blocks_per_sm(nv, ne);
         dim3 grid(sms * (bps < want ? bps : want)), block(engine::kBlockThreads);
         void *args[] = {(void *)&app, (void *)&a};
         e = cudaLaunchCooperativeKernel((const void *)kernel, grid, block, args, 0, s);
@@ -213,6 +215,11 @@ extern "C" sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *ind
     }
     const uint32_t bits = c.error | c.cnt.error;
     if (stats) {
+        stats->time_total_ms = 0;
+        stats->time_kernel_ms = 0;
+        stats->edges_reached = 0;
+        stats->vertices_reached = 0;
+        stats->search_depth = 0;
         stats->rounds = c.round;
         stats->max_iteration_reached = c.max_iteration_reached;
         for (int k = 0; k < 8; ++k) stats->rounds_by_variant[k] = c.rounds_by_variant[k];

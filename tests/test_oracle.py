@@ -143,3 +143,63 @@ def test_csr_tocsc_oracle_vs_reference():
     a = oracle.csr_tocsc(h.offsets, h.indices, h.weights)
     b = oracle.ref_csr_tocsc(h.offsets, h.indices, h.weights)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+# ---------------------------------------------------------------- full-size inputs and checkers
+@pytest.mark.parametrize("scale,sym,loops,dups", [(10, False, False, False), (12, True, False, False),
+                                                  (11, False, True, True), (16, False, False, False),
+                                                  (14, True, False, False)])
+def test_oracle_generator_equals_library_generator(scale, sym, loops, dups):
+    """The benchmark's reference arm builds its graph with the oracle's generator
+    (it must not load the library): CSR, weights and sources equal word for word."""
+    g = oracle.rmat(scale, 16, symmetric=sym, keep_self_loops=loops, keep_duplicates=dups)
+    h = sg.HostGraph.rmat(scale, 16, symmetric=sym, seed=1, keep_self_loops=loops, keep_duplicates=dups)
+    assert np.array_equal(g.offsets, h.offsets) and np.array_equal(g.indices, h.indices)
+    g.gen_weights(1, 64, 2)
+    h.gen_weights(1, 64, 2)
+    assert np.array_equal(g.weights, h.weights)
+    assert np.array_equal(g.pick_sources(8, 3), h.pick_sources(8, 3))
+    assert g.max_degree_vertex()[0] == h.max_degree_vertex()[0]
+
+
+def test_oracle_grid_equals_library_grid():
+    for r, c in ((1, 1), (1, 7), (6, 1), (7, 5), (33, 64)):
+        g, h = oracle.grid(r, c), sg.HostGraph.grid(r, c)
+        assert np.array_equal(g.offsets, h.offsets) and np.array_equal(g.indices, h.indices)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_dijkstra_equals_ssspnaive_golden(path):
+    g = _load(path)
+    assert (oracle.dijkstra(g["offsets"], g["indices"], g["weights"], int(g["source"])) == g["sssp"]).all()
+
+
+@pytest.mark.parametrize("kind", ["rmat_dir", "rmat_sym", "grid"])
+def test_dijkstra_equals_ssspnaive(kind):
+    if kind == "grid":
+        h = oracle.grid(64, 48).gen_weights(1, 1000, 2)
+    else:
+        h = oracle.rmat(14, 16, symmetric=kind == "rmat_sym").gen_weights(1, 64, 2)
+    for src in h.pick_sources(3, 7):
+        want = oracle.ref_sssp(h.offsets, h.indices, h.weights, int(src)) if oracle.ref_available() else \
+            oracle.sssp(h.offsets, h.indices, h.weights, int(src))
+        assert np.array_equal(oracle.dijkstra(h.offsets, h.indices, h.weights, int(src)), want)
+
+
+@pytest.mark.parametrize("path", GOLDEN + ["rmat14"], ids=[os.path.basename(p)[:-4] for p in GOLDEN] + ["rmat14"])
+def test_pagerank_fixed_point_equals_residual_push(path):
+    """The parallel Jacobi FP64 oracle used at full size converges to PageRankHost's
+    fixed point: it agrees with the FP64 residual-push restatement run to 1e-14."""
+    if path == "rmat14":
+        h = oracle.rmat(14, 16)
+        off, idx = h.offsets, h.indices
+    else:
+        g = _load(path)
+        off, idx = g["offsets"], g["indices"]
+    if len(off) < 2:
+        return
+    jac, sweeps = oracle.pagerank_fixed_point_f64(off, idx, 1e-14)
+    push = oracle.pagerank_f64(off, idx, 1e-14)
+    assert sweeps < 2000
+    assert np.abs(jac / jac.sum() - push / push.sum()).sum() <= 1e-11
+    assert np.allclose(jac, push, rtol=1e-9, atol=1e-12)
