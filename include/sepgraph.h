@@ -101,8 +101,13 @@ typedef struct sg_options {
                                  ReorderSafe() holds only) */
     int32_t wl_sort;          /* --wl_sort: sort the worklist of each data-driven push round by vertex id
                                  (framework.cuh:488-496); single-query calls, batches ignore it */
-    int32_t reserved[1];
+    int32_t worklist;         /* worklists of a forced SG_ASYNC_PUSH_DD run with load balancing: 0 = library
+                                 choice, SG_WORKLIST_QUEUE = deduplicated queues, SG_WORKLIST_BITMAP = the
+                                 output slot's bitmap itself (fire-and-forget bit sets, no appends) */
 } sg_options;
+#define SG_WORKLIST_AUTO 0
+#define SG_WORKLIST_QUEUE 1
+#define SG_WORKLIST_BITMAP 2
 
 /* Per-round trace record (the reference's --trace line, framework.cuh:334-348). */
 typedef struct sg_round_trace {

@@ -171,7 +171,7 @@ extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources,
     const bool push_mode = best->variant == SG_VARIANT_AUTO || best->variant == SG_ASYNC_PUSH_DD;
     {
         const sg_options cur = *best;
-        for (int b : {1, 2, 4, 8}) {
+        for (int b : {1, 2, 3, 4, 8}) {
             sg_options c = cur;
             c.blocks_per_sm = b;
             trial(c);
@@ -219,14 +219,22 @@ extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources,
     }
     if (push_mode && algo != SG_QUERY_PAGERANK) {
         // edges per chunk of a split vertex: smaller chunks spread a hub's
-        // first relaxations over more warps (SSSP on RMAT-22: 64 -> 4.02 ms,
-        // 256 -> 4.12, 1024 -> 4.69 per source)
+        // first relaxations over more warps, larger ones give each lane more
+        // edges in flight (SSSP on RMAT-22 with 8 edges per lane per step:
+        // 256 -> 2.50 ms, 512 -> 2.60 per source)
         const sg_options cur = *best;
-        for (int ce : {64, 128}) {
+        for (int ce : {64, 128, 512}) {
             sg_options c = cur;
             c.chunk_edges = ce;
             trial(c);
         }
+    }
+    if (best->variant == SG_ASYNC_PUSH_DD && best->lb_push != SG_LB_NONE && !best->wl_sort) {
+        // the two worklist kinds of a forced data-driven push
+        const sg_options cur = *best;
+        sg_options c = cur;
+        c.worklist = cur.worklist == SG_WORKLIST_BITMAP ? SG_WORKLIST_QUEUE : SG_WORKLIST_BITMAP;
+        trial(c);
     }
     if (best_ms) *best_ms = best_t;
     return SG_OK;

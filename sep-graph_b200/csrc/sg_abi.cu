@@ -130,6 +130,7 @@ sgb::EngineConfig make_config(const sg_graph *g, const sg_options &o, int scheme
     if (o.chunk_edges > 0) c.chunk_edges = (uint32_t)o.chunk_edges;
     if (o.local_depth > 0) c.local_depth = (uint32_t)o.local_depth;
     c.wl_sort = o.wl_sort != 0;
+    c.worklist = o.worklist;
     // SetSampleBasedPriority (common.h:229-233; hybrid_pr.cu:135-137 sets it when --cut_threshold > 0)
     if (o.priority == SG_PRIORITY_SAMPLING && o.cut_threshold > 0) c.sample_cut = (float)std::min(o.cut_threshold, 1.0);
     c.blocking = o.blocking != 0;

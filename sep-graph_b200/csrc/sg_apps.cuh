@@ -127,6 +127,11 @@ struct SSSP : AppBase<TValue, TBuffer, TWeight> {
         return current_priority > buffer;
     }
     __forceinline__ __device__ bool ReorderSafe() const { return true; }  // atomic monotone minimum
+    // AccumulateBuffer above is the monotone minimum of this candidate (an
+    // unreached source offers nothing: kInf never lowers a distance)
+    __forceinline__ __device__ TBuffer RelaxCandidate(index_t, index_t, TWeight weight, TBuffer buffer) const {
+        return buffer == kInf ? kInf : buffer + weight;
+    }
 };
 
 // ---------------------------------------------------------------- PageRank

@@ -706,7 +706,8 @@ sg_status prepare_batch(sg_ctx *ctx, sgb::Workspace &ws, std::vector<engine::Bat
     // team workspaces
     const uint32_t nwords = nv_max / 32 + 1;
     const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(nv_max, ne_max / std::max(1u, p.heavy_threshold)) + 2;
-    const uint32_t chunk_cap = (uint32_t)(ne_max / p.chunk_edges + heavy_cap + 2);
+    // chunks are cut on the 4-edge grid: at most one more per heavy vertex than deg / chunk_edges rounded up
+    const uint32_t chunk_cap = (uint32_t)(ne_max / p.chunk_edges + 2ull * heavy_cap + 2);
     TB *buf, *tmp;
     uint32_t *qq, *bm, *fl, *mid, *chunk, *counter;
     HeavyItem<TB> *heavy;
@@ -938,10 +939,11 @@ engine::Params batch_params(const sg_options &o, int scheme) {
     p.has_csc = 1;
     p.max_iteration = o.max_iteration > 0 ? (uint32_t)o.max_iteration : 200u;
     p.heavy_threshold = o.heavy_degree > 0 ? (uint32_t)o.heavy_degree : 32u;
-    p.chunk_edges = o.chunk_edges > 0 ? (uint32_t)std::max(32, o.chunk_edges) : 256u;
+    p.chunk_edges = o.chunk_edges > 0 ? ((uint32_t)std::max(32, o.chunk_edges) + 3u) & ~3u : 256u;
     p.pull_warp_threshold = 32;
     p.local_depth = o.local_depth > 0 ? (uint32_t)o.local_depth : 0u;
     p.sample_cut = o.priority == SG_PRIORITY_SAMPLING && o.cut_threshold > 0 ? (float)std::min(o.cut_threshold, 1.0) : 0.f;
+    p.bitmap_frontier = engine::use_bitmap_frontier(p.forced, p.lb_push, false, o.worklist);
     p.alpha = o.alpha;
     p.beta = o.beta > 0 ? o.beta : 18;
     p.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);

@@ -60,6 +60,16 @@ __device__ __forceinline__ T ld_l2(const T *p) {
     return __ldcg(p);
 }
 
+// 16-byte read-only load (ld.global.nc.v4); p must be 16-byte aligned.
+__device__ __forceinline__ uint4 ldg_v4(const uint32_t *p) { return __ldg(reinterpret_cast<const uint4 *>(p)); }
+// Load through L1 of data written earlier in the same launch by other blocks:
+// valid after a grid barrier, whose acquire (thread 0) and __syncthreads order
+// this SM's later loads after every block's earlier writes.
+template <typename T>
+__device__ __forceinline__ T ld_l1(const T *p) {
+    return __ldca(p);
+}
+
 __device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x) {
     const uint32_t lane = lane_id();
 #pragma unroll
@@ -107,6 +117,14 @@ __device__ __forceinline__ bool bitmap_set(uint32_t *bm, uint32_t v) {
     return (atomicOr(bm + (v >> 5), bit) & bit) == 0;
 }
 __device__ __forceinline__ void bitmap_clear(uint32_t *bm, uint32_t v) { atomicAnd(bm + (v >> 5), ~(1u << (v & 31u))); }
+// Sets the bit without returning the old word: a fire-and-forget reduction
+// the issuing thread never waits for.
+__device__ __forceinline__ void bitmap_set_nr(uint32_t *bm, uint32_t v) {
+    asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(bm + (v >> 5)), "r"(1u << (v & 31u)) : "memory");
+}
+__device__ __forceinline__ void red_add(uint32_t *p, uint32_t v) {
+    asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // Bounded grid barrier for a cooperative launch (all blocks co-resident).
 // The last block to arrive runs `leader()` on one thread with every block's

@@ -93,6 +93,7 @@ struct Counters {
     uint32_t active_count;  // active vertices of a round whose worklist nobody reads (forced TD)
     uint32_t heavy_count[2], chunk_count[2];  // heavy-vertex tables, one set per round parity
     unsigned long long edges_processed;
+    uint32_t popped;  // worklist items taken from a bitmap worklist this round
 };
 
 struct Ctrl {
@@ -120,11 +121,26 @@ struct Params {
     uint32_t pull_warp_threshold;
     uint32_t local_depth;  // levels a block follows its own discoveries inside a push round (0 = off)
     float sample_cut;      // sampling priority in ASYNC_PUSH_TD rounds (SetSampleBasedPriority), 0 = off
+    // Bitmap worklists (forced ASYNC_PUSH_DD with load balancing, worklists
+    // unsorted): a push sets the destination's bit in the output slot's queued
+    // bitmap with a fire-and-forget reduction and appends nothing; the next
+    // round takes its items from that bitmap (see push_phase_a).  The slot
+    // counters then count pushes, not distinct vertices (zero iff empty).
+    int32_t bitmap_frontier;
     double alpha, beta;
     long long total_workload0;
     unsigned long long prio_init_raw, prio_step_raw;
     unsigned long long timeout_ns;
 };
+
+// Bitmap worklists are used when every round is a forced ASYNC_PUSH_DD with
+// load balancing and the worklists need not be sorted (--wl_sort builds a
+// sorted queue instead).
+// worklist: SG_WORKLIST_AUTO / _QUEUE / _BITMAP (sg_options.worklist).
+inline bool use_bitmap_frontier(int forced, int lb_push, bool wl_sort, int worklist) {
+    if (forced != V_ASYNC_PUSH_DD || lb_push == LB_NONE || wl_sort) return false;
+    return worklist == SG_WORKLIST_BITMAP;
+}
 
 template <typename TValue, typename TBuffer, typename TWeight>
 struct KArgs {
@@ -151,7 +167,17 @@ struct KArgs {
     Params p;
     // --wl_sort: one count per block of the team; null = worklists are not sorted
     uint32_t *sort_counts = nullptr;
+    // Edge-tiled topology-driven pull (functors with PullReduce, unweighted):
+    // tile_row[t] = the in-edge row holding CSC edge t * kPullTileEdges
+    // (ceil(E / kPullTileEdges) + 1 entries, the last = V - 1), filled at the
+    // launch's start; null = the destination-per-lane pull is used instead.
+    uint32_t *tile_row = nullptr;
 };
+
+// In-edges per warp tile of the edge-tiled pull: 8 per lane, two 16-byte loads.
+constexpr uint32_t kPullTileEdges = 256;
+// Rows a tile may span and still sum its rows in shared memory first.
+constexpr uint32_t kPullTileRows = 64;
 
 // Leader-only policy state (RunningInfo), lives in block 0 / thread 0.
 struct PolicyState {
@@ -177,6 +203,12 @@ struct WarpLB {
     // topology-driven pull: each lane's first and last (possibly shared) segment
     uint32_t partk[2][32];
     TBuffer part[2][32];
+    // edge-tiled pull: per-row sums of one tile and the rows touched
+    TBuffer rowsum[kPullTileRows];
+    unsigned long long touched;
+    // bitmap worklist: the 32 words a warp took and their exclusive popcount scan
+    uint32_t scan_excl[32];
+    uint32_t scan_bits[32];
 };
 
 // A block's own queue of vertices it discovered in a push round and may
@@ -263,6 +295,43 @@ __device__ __forceinline__ bool reorder_safe(const App &app) {
         return app.ReorderSafe();
     else
         return false;
+}
+
+// Optional functor extension (no reference counterpart): a functor whose
+// weighted AccumulateBuffer is exactly a monotone minimum,
+//   cand = RelaxCandidate(src, dst, weight, offered);
+//   if (cand < *p_buffer) { atomicMin(p_buffer, cand); return SUCCESS_CONTINUE; }
+//   return FAILURE_CONTINUE;
+// over an unsigned integer buffer, declares
+//   __device__ TBuffer RelaxCandidate(index_t src, index_t dst, TWeight w, TBuffer offered) const
+// and the engine relaxes hub chunks eight edges per lane at a time: the eight
+// current values are loaded together and only improving minima are issued.
+// IsHighPriority of such a functor must hold for every value at or below one
+// it holds for (a smaller buffer is never of lower priority): the engine then
+// routes a push by its candidate instead of re-reading the destination.
+template <typename App, typename TB, typename TW, typename = void>
+struct has_min_relax : std::false_type {};
+template <typename App, typename TB, typename TW>
+struct has_min_relax<App, TB, TW,
+                     std::void_t<decltype(std::declval<const App &>().RelaxCandidate(
+                         std::declval<uint32_t>(), std::declval<uint32_t>(), std::declval<TW>(), std::declval<TB>()))>>
+    : std::integral_constant<bool, std::is_same<TB, uint32_t>::value> {};
+
+// Edge range of chunk k of a heavy vertex's list [beg, beg + deg): chunks are
+// cut on the 4-edge grid (from beg rounded down to a multiple of 4) so that
+// every chunk starts on a 16-byte boundary of the edge arrays, which lets a
+// lane read its edges with 16-byte loads; the first chunk starts at beg.
+__host__ __device__ __forceinline__ uint32_t chunk_count_of(uint32_t beg, uint32_t deg, uint32_t ce) {
+    const uint32_t a0 = beg & ~3u;
+    return (beg + deg - a0 + ce - 1) / ce;
+}
+__host__ __device__ __forceinline__ void chunk_span(uint32_t beg, uint32_t deg, uint32_t ce, uint32_t k,
+                                                    uint32_t *lo, uint32_t *hi) {
+    const uint32_t a0 = beg & ~3u;
+    const uint32_t s = a0 + k * ce;
+    *lo = s > beg ? s : beg;
+    const uint32_t e = s + ce, end = beg + deg;
+    *hi = e < end ? e : end;
 }
 
 // Dispatch to the weighted or unweighted AccumulateBuffer overload like
@@ -405,10 +474,11 @@ struct EngineKernel {
     // With a block queue `lq`, near (high-priority) vertices go there first.
     // All 32 lanes must call.
     static __device__ __forceinline__ void enqueue(App &app, const Args &a, const Snap &s, uint32_t dst, bool want,
-                                                   Acc &acc, LocalQ *lq = nullptr) {
+                                                   Acc &acc, LocalQ *lq = nullptr, const TB *offered = nullptr) {
         Counters *n = &a.ctrl->cnt;
         bool hi = true;
-        if (a.p.priority && want) hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), dev::ld_l2(a.buffer + dst));
+        if (a.p.priority && want)
+            hi = app.App::IsHighPriority(from_raw<TB>(s.prio_raw), offered ? *offered : dev::ld_l2(a.buffer + dst));
         if (lq) {
             bool loc = want && hi;
             const uint32_t m = __ballot_sync(dev::kFullMask, loc);
@@ -428,11 +498,119 @@ struct EngineKernel {
             want = want && !loc;
         }
         bool w_hi = want && hi, w_lo = want && !hi;
+        if (a.p.bitmap_frontier) {
+            // no dedupe round trip and no append: the bit is the worklist entry
+            if (w_hi) dev::bitmap_set_nr(a.qflag[s.qhi], dst);
+            if (w_lo) dev::bitmap_set_nr(a.qflag[s.qlo], dst);
+            count_pushes(n, s, w_hi, w_lo);
+            if (w_hi || w_lo) count_enq(a, acc, w_hi, dst);
+            return;
+        }
         if (w_hi) w_hi = dev::bitmap_set(a.qflag[s.qhi], dst);
         if (w_lo) w_lo = dev::bitmap_set(a.qflag[s.qlo], dst);
         dev::warp_append(a.queue[s.qhi], &n->qcount[s.qhi], a.queue_cap, w_hi, dst, &n->error);
         if (a.p.priority) dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, w_lo, dst, &n->error);
         if (w_hi || w_lo) count_enq(a, acc, w_hi, dst);
+    }
+
+    // Bitmap worklists: one fire-and-forget add per warp and slot of the
+    // number of pushes (the leader only needs to know whether a slot is empty).
+    // All 32 lanes must call.
+    static __device__ __forceinline__ void count_pushes(Counters *n, const Snap &s, bool w_hi, bool w_lo) {
+        const uint32_t mh = __ballot_sync(dev::kFullMask, w_hi), ml = __ballot_sync(dev::kFullMask, w_lo);
+        if (dev::lane_id() == 0) {
+            if (mh) dev::red_add(&n->qcount[s.qhi], (uint32_t)__popc(mh));
+            if (ml) dev::red_add(&n->qcount[s.qlo], (uint32_t)__popc(ml));
+        }
+    }
+
+    // K pushes per lane at once, with the candidate values the pushes offer
+    // (the priority routing uses them, see has_min_relax; null = read each
+    // destination's buffer as enqueue() does).  Same effect as K
+    // enqueue() calls, but the K queued-bit updates are issued together and
+    // each slot gets one warp-wide reservation for all of them: two dependent
+    // memory round trips per call instead of two per push.  All 32 lanes must
+    // call.
+    template <int K>
+    static __device__ __forceinline__ void enqueue_batch(App &app, const Args &a, const Snap &s, const uint32_t *dst,
+                                                         bool *want, const TB *offered, Acc &acc, LocalQ *lq) {
+        Counters *n = &a.ctrl->cnt;
+        const TB prio = from_raw<TB>(s.prio_raw);
+        bool hi[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            hi[j] = !a.p.priority || !want[j] ||
+                    app.App::IsHighPriority(prio, offered ? offered[j] : dev::ld_l2(a.buffer + dst[j]));
+        if (lq) {  // near vertices go to the block's lookahead queue first
+            const uint32_t lane = dev::lane_id();
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                bool loc = want[j] && hi[j];
+                const uint32_t m = __ballot_sync(dev::kFullMask, loc);
+                if (m) {
+                    const uint32_t leader = __ffs(m) - 1, o = lq->out;
+                    uint32_t base = 0;
+                    if (lane == leader) base = atomicAdd(&lq->n[o], (uint32_t)__popc(m));
+                    base = __shfl_sync(dev::kFullMask, base, leader);
+                    if (loc) {
+                        const uint32_t pos = base + __popc(m & dev::lanemask_lt());
+                        if (pos < kLocalCap)
+                            lq->item[o][pos] = dst[j];
+                        else
+                            loc = false;
+                    }
+                }
+                want[j] = want[j] && !loc;
+            }
+        }
+        if (a.p.bitmap_frontier) {
+            uint32_t ch = 0, cl = 0;
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (want[j]) {
+                    dev::bitmap_set_nr(a.qflag[hi[j] ? s.qhi : s.qlo], dst[j]);
+                    count_enq(a, acc, hi[j], dst[j]);
+                }
+                ch += want[j] && hi[j];
+                cl += want[j] && !hi[j];
+            }
+            ch = dev::warp_sum(ch);
+            cl = dev::warp_sum(cl);
+            if (dev::lane_id() == 0) {
+                if (ch) dev::red_add(&n->qcount[s.qhi], ch);
+                if (cl) dev::red_add(&n->qcount[s.qlo], cl);
+            }
+            return;
+        }
+        bool w[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) w[j] = want[j] ? dev::bitmap_set(a.qflag[hi[j] ? s.qhi : s.qlo], dst[j]) : false;
+        uint32_t ch = 0, cl = 0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            ch += w[j] && hi[j];
+            cl += w[j] && !hi[j];
+        }
+        const uint32_t ih = dev::warp_inclusive_scan(ch), il = dev::warp_inclusive_scan(cl);
+        const uint32_t th = __shfl_sync(dev::kFullMask, ih, 31), tl = __shfl_sync(dev::kFullMask, il, 31);
+        uint32_t bh = 0, bl = 0;
+        if (dev::lane_id() == 0) {
+            if (th) bh = atomicAdd(&n->qcount[s.qhi], th);
+            if (tl) bl = atomicAdd(&n->qcount[s.qlo], tl);
+        }
+        bh = __shfl_sync(dev::kFullMask, bh, 0) + ih - ch;
+        bl = __shfl_sync(dev::kFullMask, bl, 0) + il - cl;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (!w[j]) continue;
+            const uint32_t q = hi[j] ? s.qhi : s.qlo;
+            const uint32_t pos = hi[j] ? bh++ : bl++;
+            if (pos < a.queue_cap)
+                a.queue[q][pos] = dst[j];
+            else
+                atomicOr(&n->error, dev::kErrCapacity);
+            count_enq(a, acc, hi[j], dst[j]);
+        }
     }
 
     // Single-thread enqueue (LB NONE paths run divergent per-thread loops).
@@ -468,7 +646,7 @@ struct EngineKernel {
         Counters *n = &a.ctrl->cnt;
         const uint32_t lane = dev::lane_id();
         const uint32_t ce = a.p.chunk_edges;
-        const uint32_t nch = heavy ? (deg + ce - 1) / ce : 0u;
+        const uint32_t nch = heavy ? chunk_count_of(beg, deg, ce) : 0u;
         const uint32_t incl = dev::warp_inclusive_scan(nch);
         const uint32_t tot = __shfl_sync(dev::kFullMask, incl, 31);
         const uint32_t leader = __ffs(m) - 1;
@@ -522,19 +700,52 @@ struct EngineKernel {
         w.src[lane] = src;
         w.pay[lane] = payload;
         __syncwarp();
-        // Two-stage software pipeline: the next batch's owner lookup, index and
-        // weight loads (and an L2 prefetch of its destination state) are issued
-        // before the current batch's accumulate/enqueue chain.
-        EdgeRef cur = locate(a, w, lane, total);
-        for (uint32_t eb = 0; eb < total; eb += 32) {
-            const EdgeRef nxt = locate(a, w, eb + 32 + lane, total);
-            bool want = false;
-            if (cur.valid) {
-                const int st = accumulate_w(app, cur.src, cur.dst, cur.wt, a.buffer + cur.dst, cur.pay);
-                want = dd && acc_success(st);
+        if constexpr (has_min_relax<App, TB, TW>::value) {
+            // Min-relax functors: 4 edges per lane per step (edge eb + 32j + lane),
+            // their 4 destination values loaded together, one batched push.
+            for (uint32_t eb = 0; eb < total; eb += 128) {
+                EdgeRef r[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) r[j] = locate(a, w, eb + 32u * j + lane, total);
+                uint32_t d[4];
+                TB cand[4], cur[4];
+                bool want[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    d[j] = r[j].dst;
+                    cand[j] = r[j].valid ? app.RelaxCandidate(r[j].src, r[j].dst, (TW)r[j].wt, r[j].pay)
+                                         : std::numeric_limits<TB>::max();
+                    cur[j] = r[j].valid ? dev::ld_l2(a.buffer + r[j].dst) : (TB)0;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    want[j] = cand[j] < cur[j];
+                    if (want[j]) atomicMin(a.buffer + d[j], cand[j]);
+                    want[j] = want[j] && dd;
+                }
+                enqueue_batch<4>(app, a, s, d, want, cand, acc, lq);
             }
-            enqueue(app, a, s, cur.dst, want, acc, lq);
-            cur = nxt;
+        } else {
+            // 4 edges per lane per step (edge eb + 32j + lane): their owner lookups
+            // and index/weight loads, then the 4 accumulations, then one batched
+            // push, so a lane has 4 independent memory chains in flight.
+            for (uint32_t eb = 0; eb < total; eb += 128) {
+                EdgeRef r[4];
+    #pragma unroll
+                for (int j = 0; j < 4; ++j) r[j] = locate(a, w, eb + 32u * j + lane, total);
+                uint32_t d[4];
+                bool want[4];
+    #pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    d[j] = r[j].dst;
+                    want[j] = false;
+                    if (r[j].valid) {
+                        const int st = accumulate_w(app, r[j].src, r[j].dst, r[j].wt, a.buffer + r[j].dst, r[j].pay);
+                        want[j] = dd && acc_success(st);
+                    }
+                }
+                enqueue_batch<4>(app, a, s, d, want, nullptr, acc, lq);
+            }
         }
         if (lane == 0) acc.edges += total;
         __syncwarp();
@@ -597,6 +808,14 @@ struct EngineKernel {
 
     // Chunks of the heavy vertices registered in table `set`, spread over all warps.
     static __device__ void heavy_phase(App &app, const Args &a, const Snap &s, uint32_t set, bool dd, Acc &acc) {
+        if constexpr (has_min_relax<App, TB, TW>::value)
+            heavy_phase_relax(app, a, s, set, dd, acc);
+        else
+            heavy_phase_generic(app, a, s, set, dd, acc);
+    }
+
+    static __device__ void heavy_phase_generic(App &app, const Args &a, const Snap &s, uint32_t set, bool dd,
+                                               Acc &acc) {
         const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count[set]), a.chunk_cap);
         const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count[set]), a.heavy_cap);
         const uint32_t *own = a.chunk_owner + (size_t)set * a.chunk_cap;
@@ -608,35 +827,116 @@ struct EngineKernel {
             if (e >= H) continue;
             const HeavyItem<TB> h = items[e];
             if (ch < h.chunk_base) continue;
-            const uint32_t off = (ch - h.chunk_base) * ce;
-            if (off >= h.deg) continue;
-            const uint32_t len = min(ce, h.deg - off);
-            auto load = [&](uint32_t i, uint32_t &dst, uint32_t &wt) {
-                dst = 0;
-                wt = 1;
-                if (i < len) {
-                    const uint32_t edge = h.beg + off + i;
-                    dst = a.csr.edge_dest(edge);
-                    if constexpr (!std::is_same<TW, graphs::NoWeight>::value)
-                        if (a.csr_w) wt = __ldg(a.csr_w + edge);
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.buffer + dst));
+            uint32_t lo, hi;
+            chunk_span(h.beg, h.deg, ce, ch - h.chunk_base, &lo, &hi);
+            if (lo >= hi) continue;
+            const uint32_t off = lo - h.beg;
+            const uint32_t len = hi - lo;
+            for (uint32_t k = 0; k < len; k += 128) {
+                uint32_t d[4], wt[4];
+                bool want[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint32_t i = k + 32u * j + lane;
+                    d[j] = 0;
+                    wt[j] = 1;
+                    if (i < len) {
+                        const uint32_t edge = h.beg + off + i;
+                        d[j] = a.csr.edge_dest(edge);
+                        if constexpr (!std::is_same<TW, graphs::NoWeight>::value)
+                            if (a.csr_w) wt[j] = __ldg(a.csr_w + edge);
+                    }
                 }
-            };
-            uint32_t dst, wt;
-            load(lane, dst, wt);
-            for (uint32_t k = 0; k < len; k += 32) {
-                uint32_t ndst, nwt;
-                load(k + 32 + lane, ndst, nwt);
-                bool want = false;
-                if (k + lane < len) {
-                    const int st = accumulate_w(app, h.src, dst, wt, a.buffer + dst, h.payload);
-                    want = dd && acc_success(st);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    want[j] = false;
+                    if (k + 32u * j + lane < len) {
+                        const int st = accumulate_w(app, h.src, d[j], wt[j], a.buffer + d[j], h.payload);
+                        want[j] = dd && acc_success(st);
+                    }
                 }
-                enqueue(app, a, s, dst, want, acc);
-                dst = ndst;
-                wt = nwt;
+                enqueue_batch<4>(app, a, s, d, want, nullptr, acc, nullptr);
             }
             if (lane == 0) acc.edges += len;
+        }
+    }
+
+    // Hub chunks of a min-relax functor: lane l takes the 8 edge slots
+    // [w + 8l, w + 8l + 8) of each 256-slot window w of the chunk (two 16-byte
+    // loads each of destinations and weights; windows start on the chunk
+    // grid's 16-byte boundaries), loads the 8 current destination values
+    // together, issues the improving minima as reductions and pushes the
+    // improved destinations.  The next chunk's owner entry is loaded while
+    // the current chunk relaxes.
+    static __device__ void heavy_phase_relax(App &app, const Args &a, const Snap &s, uint32_t set, bool dd,
+                                             Acc &acc) {
+        if constexpr (has_min_relax<App, TB, TW>::value) {
+            const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count[set]), a.chunk_cap);
+            const uint32_t H = min(dev::ld_l2(&a.ctrl->cnt.heavy_count[set]), a.heavy_cap);
+            const uint32_t *own = a.chunk_owner + (size_t)set * a.chunk_cap;
+            const HeavyItem<TB> *items = a.heavy + (size_t)set * a.heavy_cap;
+            const uint32_t lane = dev::lane_id();
+            const uint32_t ce = a.p.chunk_edges;
+            const uint32_t E = a.csr.nedges;
+            const uint32_t *col = a.csr.edge_dst;
+            const uint32_t *wts = a.csr_w;
+            const bool vec = (reinterpret_cast<uintptr_t>(col) & 15u) == 0 &&
+                             (reinterpret_cast<uintptr_t>(wts) & 15u) == 0;
+            const uint32_t nw = nwarps();
+            uint32_t ch = gwarp();
+            uint32_t e_next = ch < C ? dev::ld_l2(own + ch) : 0xffffffffu;
+            for (; ch < C; ch += nw) {
+                const uint32_t e = e_next;
+                e_next = ch + nw < C ? dev::ld_l2(own + ch + nw) : 0xffffffffu;
+                if (e >= H) continue;
+                const HeavyItem<TB> h = items[e];
+                if (ch < h.chunk_base) continue;
+                uint32_t lo, hi;
+                chunk_span(h.beg, h.deg, ce, ch - h.chunk_base, &lo, &hi);
+                if (lo >= hi) continue;
+                for (uint32_t w0 = lo & ~3u; w0 < hi; w0 += 256u) {
+                    const uint32_t base = w0 + lane * 8u;
+                    uint32_t d[8], wt[8];
+                    if (vec && base + 8u <= E) {
+                        const uint4 x = dev::ldg_v4(col + base), y = dev::ldg_v4(col + base + 4);
+                        d[0] = x.x, d[1] = x.y, d[2] = x.z, d[3] = x.w, d[4] = y.x, d[5] = y.y, d[6] = y.z, d[7] = y.w;
+                        if (wts) {
+                            const uint4 p = dev::ldg_v4(wts + base), q = dev::ldg_v4(wts + base + 4);
+                            wt[0] = p.x, wt[1] = p.y, wt[2] = p.z, wt[3] = p.w, wt[4] = q.x, wt[5] = q.y, wt[6] = q.z,
+                            wt[7] = q.w;
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) wt[j] = 1u;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const uint32_t i = base + j;
+                            const bool in = i >= lo && i < hi;
+                            d[j] = in ? __ldg(col + i) : 0u;
+                            wt[j] = in && wts ? __ldg(wts + i) : 1u;
+                        }
+                    }
+                    TB cand[8], cur[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t i = base + j;
+                        const bool in = i >= lo && i < hi;
+                        cand[j] = in ? app.RelaxCandidate(h.src, d[j], (TW)wt[j], h.payload)
+                                     : std::numeric_limits<TB>::max();
+                        cur[j] = in ? dev::ld_l2(a.buffer + d[j]) : (TB)0;
+                    }
+                    bool want[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        want[j] = cand[j] < cur[j];
+                        if (want[j]) atomicMin(a.buffer + d[j], cand[j]);
+                        want[j] = want[j] && dd;
+                    }
+                    enqueue_batch<8>(app, a, s, d, want, cand, acc, nullptr);
+                }
+                if (lane == 0) acc.edges += hi - lo;
+            }
         }
     }
 
@@ -770,35 +1070,114 @@ struct EngineKernel {
         __syncthreads();
     }
 
+    // The r-th (from 0) set bit of x; r < popc(x).
+    static __device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t r) {
+        uint32_t pos = 0;
+#pragma unroll
+        for (uint32_t w = 16; w > 0; w >>= 1) {
+            const uint32_t lo = __popc(x & ((1u << w) - 1u));
+            if (r >= lo) {
+                r -= lo;
+                x >>= w;
+                pos += w;
+            } else {
+                x &= (1u << w) - 1u;
+            }
+        }
+        return pos;
+    }
+
     static __device__ void push_phase_a(App &app, const Args &a, const Snap &s, WarpLB<TB> &wlb, bool dd,
                                         int lb, Acc &acc, LocalQ *lq = nullptr) {
         const uint32_t lane = dev::lane_id();
         const uint32_t N = dd ? s.F : a.csr.nnodes;
         const uint32_t *Q = a.queue[s.qin];
+        if (dd && a.p.bitmap_frontier) {
+            // The worklist is the input slot's bitmap.  A warp takes 32 words
+            // spread evenly over the vertex range (word gw + k * nwarps for lane
+            // k), so every warp samples every region of the id space (RMAT
+            // graphs put their dense rows at low ids); it clears the words it
+            // took (no other writer touches the input slot this round), ranks
+            // their set bits with one warp scan and processes them 32 at a time
+            // exactly like queue items.
+            uint32_t *bits = a.qflag[s.qin];
+            const uint32_t W = a.nwords, nw = nwarps();
+            uint32_t popped = 0;
+            for (uint32_t b = gwarp(); b < W; b += 32u * nw) {
+                const uint32_t wi = b + lane * nw;
+                uint32_t x = 0;
+                if (wi < W) {
+                    x = dev::ld_l2(bits + wi);
+                    if (x) bits[wi] = 0u;
+                }
+                const uint32_t c = __popc(x);
+                const uint32_t incl = dev::warp_inclusive_scan(c);
+                const uint32_t total = __shfl_sync(dev::kFullMask, incl, 31);
+                popped += c;
+                if (total == 0) continue;
+                wlb.scan_excl[lane] = incl - c;
+                wlb.scan_bits[lane] = x;
+                __syncwarp();
+                for (uint32_t g0 = 0; g0 < total; g0 += 32) {
+                    const uint32_t r = g0 + lane;
+                    const bool valid = r < total;
+                    uint32_t v = 0;
+                    if (valid) {
+                        const uint32_t k = owner(wlb.scan_excl, r);
+                        v = (b + k * nw) * 32u + nth_set_bit(wlb.scan_bits[k], r - wlb.scan_excl[k]);
+                    }
+                    push_item(app, a, s, wlb, true, lb, acc, lq, v, valid, false);
+                }
+                __syncwarp();
+            }
+            popped = dev::warp_sum(popped);
+            if (lane == 0 && popped) dev::red_add(&a.ctrl->cnt.popped, popped);
+        } else {
+            for (uint32_t base = gwarp() * 32; base < N; base += nwarps() * 32) {
+                const uint32_t i = base + lane;
+                const bool valid = i < N;
+                uint32_t v = 0;
+                if (valid) v = dd ? dev::ld_l2(Q + i) : i;
+                push_item(app, a, s, wlb, dd, lb, acc, lq, v, valid, dd);
+            }
+        }
+        if (lq) local_levels(app, a, s, wlb, lb, acc, lq);
+    }
+
+    // One worklist item per lane (valid lanes): pop (queue worklists), far-pile
+    // check, combine, heavy registration and the warp's expansion.  All 32
+    // lanes must call.
+    static __device__ __forceinline__ void push_item(App &app, const Args &a, const Snap &s, WarpLB<TB> &wlb,
+                                                     bool dd, int lb, Acc &acc, LocalQ *lq, uint32_t v, bool valid,
+                                                     bool pop) {
         const TB prio = from_raw<TB>(s.prio_raw);
         Counters *n = &a.ctrl->cnt;
-        for (uint32_t base = gwarp() * 32; base < N; base += nwarps() * 32) {
-            const uint32_t i = base + lane;
-            const bool valid = i < N;
-            uint32_t v = 0;
+        {
             bool proceed = valid;
             bool keep = false;
             if (valid) {
-                v = dd ? dev::ld_l2(Q + i) : i;
                 // sampling priority: a topology-driven round takes only the
                 // vertices above this round's sampled threshold (driver.cuh:362-383)
                 if (!dd && a.p.sample_cut > 0.f) proceed = app.App::IsHighPriority(prio, dev::ld_l2(a.buffer + v));
                 if (dd) {
-                    dev::bitmap_clear(a.qflag[s.qin], v);  // pop
+                    if (pop) dev::bitmap_clear(a.qflag[s.qin], v);  // pop
                     if (s.pile && !app.App::IsHighPriority(prio, dev::ld_l2(a.buffer + v))) {
                         // far pile: vertices still outside the priority window move to the new pile
-                        keep = dev::bitmap_set(a.qflag[s.qlo], v);
+                        if (a.p.bitmap_frontier) {
+                            dev::bitmap_set_nr(a.qflag[s.qlo], v);
+                            keep = true;
+                        } else {
+                            keep = dev::bitmap_set(a.qflag[s.qlo], v);
+                        }
                         proceed = false;
                     }
                 }
             }
             if (dd && s.pile) {
-                dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, keep, v, &n->error);
+                if (a.p.bitmap_frontier)
+                    count_pushes(n, s, false, keep);
+                else
+                    dev::warp_append(a.queue[s.qlo], &n->qcount[s.qlo], a.queue_cap, keep, v, &n->error);
                 if (keep) count_enq(a, acc, false, v);
             }
             // the row offsets are read-only: load them alongside the combine's
@@ -818,14 +1197,13 @@ struct EngineKernel {
             uint32_t deg = sched ? end - beg : 0u;
             if (lb == LB_NONE) {
                 if (deg) expand_serial(app, a, s, v, beg, deg, payload, dd, acc, lq);
-                continue;
+                return;
             }
             const bool heavy = deg > a.p.heavy_threshold;
             register_heavy(a, s.round & 1u, heavy, v, beg, deg, payload);
             if (heavy) deg = 0;
             expand_warp(app, a, s, wlb, v, beg, deg, payload, dd, acc, lq);
         }
-        if (lq) local_levels(app, a, s, wlb, lb, acc, lq);
     }
 
     // Local lookahead: the block processes the vertices it discovered itself,
@@ -1086,6 +1464,109 @@ struct EngineKernel {
         }
     }
 
+    // Largest row r in [lo, hi] with col_start[r] <= e: the in-edge row that
+    // holds CSC edge e (empty rows share their start with the next row, so the
+    // largest such r is the non-empty one).
+    static __device__ __forceinline__ uint32_t row_of(const uint32_t *crow, uint32_t lo, uint32_t hi, uint32_t e) {
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo + 1) / 2;
+            if (__ldg(crow + mid) <= e)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return lo;
+    }
+
+    // tile_row[] of the edge-tiled pull, once per launch (all threads of the team).
+    static __device__ void compute_tile_rows(const Args &a) {
+        const uint32_t V = a.csc.nnodes, E = a.csc.nedges;
+        const uint32_t T = (E + kPullTileEdges - 1) / kPullTileEdges;
+        for (uint32_t t = gthread(); t <= T; t += nthreads())
+            a.tile_row[t] = (t == T || V == 0) ? (V ? V - 1 : 0) : row_of(a.csc.col_start, 0, V - 1, t * kPullTileEdges);
+    }
+
+    // Topology-driven pull for functors with PullReduce, tiled over the in-edge
+    // array instead of over destinations: a warp takes 256 consecutive CSC
+    // edges (8 per lane, two 16-byte index loads, 8 independent gathers of
+    // the sources' pulled values in flight per lane), finds each edge's
+    // destination row from the tile's row range, folds runs of one row in
+    // registers, sums the tile's rows in shared memory and issues one
+    // AccumulateBuffer per (row, tile).  Rows of any in-degree need no
+    // separate chunk phase: a long row is simply spread over many tiles.
+    // The pulled values were written by the combine phase of this round
+    // (before a grid barrier), so they are read through L1, where the
+    // contributions of high out-degree sources stay resident.
+    static __device__ void pull_tiles(App &app, const Args &a, WarpLB<TB> &w, Acc &acc) {
+        if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value) {
+            const uint32_t lane = dev::lane_id();
+            const uint32_t V = a.csc.nnodes, E = a.csc.nedges;
+            const uint32_t T = (E + kPullTileEdges - 1) / kPullTileEdges;
+            const uint32_t *crow = a.csc.col_start;
+            const uint32_t *srcs = a.csc.edge_source;
+            const bool aligned = (reinterpret_cast<uintptr_t>(srcs) & 15u) == 0;
+            const TB *vals = a.tmp;
+            const TB idn = app.PullIdentity();
+            for (uint32_t t = gwarp(); t < T; t += nwarps()) {
+                const uint32_t e0 = t * kPullTileEdges + lane * 8u;
+                uint32_t s[8];
+                if (aligned && e0 + 8u <= E) {
+                    const uint4 x = dev::ldg_v4(srcs + e0), y = dev::ldg_v4(srcs + e0 + 4);
+                    s[0] = x.x, s[1] = x.y, s[2] = x.z, s[3] = x.w, s[4] = y.x, s[5] = y.y, s[6] = y.z, s[7] = y.w;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) s[j] = e0 + j < E ? __ldg(srcs + e0 + j) : 0u;
+                }
+                TB g[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) g[j] = e0 + j < E ? dev::ld_l1(vals + s[j]) : idn;
+                const uint32_t rlo = __ldg(a.tile_row + t), rhi = __ldg(a.tile_row + t + 1);
+                const bool in_smem = rhi - rlo < kPullTileRows;
+                if (in_smem) {
+                    for (uint32_t k = lane; k <= rhi - rlo; k += 32) w.rowsum[k] = idn;
+                    if (lane == 0) w.touched = 0ull;
+                    __syncwarp();
+                }
+                auto flush = [&](uint32_t r, TB v) {
+                    if (in_smem) {
+                        atomicAdd(&w.rowsum[r - rlo], v);  // shared-memory reduction of the tile's rows
+                        atomicOr(&w.touched, 1ull << (r - rlo));
+                    } else {
+                        accumulate<App, TB, TW>(app, a.csc_w, r, r, 0, a.buffer + r, v);
+                    }
+                };
+                if (e0 < E) {
+                    uint32_t r = row_of(crow, rlo, rhi, e0);
+                    uint32_t next = r + 1 < V ? __ldg(crow + r + 1) : E;
+                    TB run = idn;
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t e = e0 + j;
+                        if (e < E) {
+                            if (e >= next) {
+                                flush(r, run);
+                                run = idn;
+                                r = row_of(crow, r + 1, rhi, e);
+                                next = r + 1 < V ? __ldg(crow + r + 1) : E;
+                            }
+                            run = app.PullReduce(run, g[j]);
+                        }
+                    }
+                    flush(r, run);
+                }
+                if (in_smem) {
+                    __syncwarp();
+                    const unsigned long long m = w.touched;
+                    for (uint32_t k = lane; k <= rhi - rlo; k += 32)
+                        if ((m >> k) & 1ull) accumulate<App, TB, TW>(app, a.csc_w, rlo + k, rlo + k, 0, a.buffer + rlo + k,
+                                                                    w.rowsum[k]);
+                    __syncwarp();
+                }
+                if (lane == 0) acc.edges += min(kPullTileEdges, E - t * kPullTileEdges);
+            }
+        }
+    }
+
     static __device__ void pull_reduce_chunks(App &app, const Args &a, uint32_t set, Acc &acc) {
         if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, graphs::NoWeight>::value) {
             const uint32_t C = min(dev::ld_l2(&a.ctrl->cnt.chunk_count[set]), a.chunk_cap);
@@ -1099,12 +1580,13 @@ struct EngineKernel {
                 if (e >= H) continue;
                 const HeavyItem<TB> h = items[e];
                 if (ch < h.chunk_base) continue;
-                const uint32_t off = (ch - h.chunk_base) * ce;
-                if (off >= h.deg) continue;
-                const uint32_t len = min(ce, h.deg - off);
+                uint32_t lo, hi;
+                chunk_span(h.beg, h.deg, ce, ch - h.chunk_base, &lo, &hi);
+                if (lo >= hi) continue;
+                const uint32_t len = hi - lo;
                 TB r = app.PullIdentity();
                 for (uint32_t k = lane; k < len; k += 32)
-                    r = app.PullReduce(r, dev::ld_l2(a.tmp + a.csc.edge_src(h.beg + off + k)));
+                    r = app.PullReduce(r, dev::ld_l2(a.tmp + a.csc.edge_src(lo + k)));
 #pragma unroll
                 for (int d = 16; d > 0; d >>= 1) r = app.PullReduce(r, __shfl_xor_sync(dev::kFullMask, r, d));
                 if (lane == 0) {
@@ -1266,7 +1748,8 @@ struct EngineKernel {
         ps.rounds_by_variant[var & 7]++;
         const unsigned long long now = dev::globaltimer_ns();
         const float round_ms = (float)(now - ps.t_round_start) * 1e-6f;
-        ps.vertices_processed += is_dd(var) ? rs.F : a.csr.nnodes;
+        ps.vertices_processed += !is_dd(var) ? a.csr.nnodes
+                                 : (a.p.bitmap_frontier && var == V_ASYNC_PUSH_DD) ? dev::ld_l2(&n->popped) : rs.F;
         const bool prio_push = a.p.priority && var == V_ASYNC_PUSH_DD;
         const uint32_t out_hi = count_only(a) ? dev::ld_l2(&n->active_count) : qc[rs.qhi];
         const uint32_t out_lo = prio_push ? qc[rs.qlo] : 0;
@@ -1345,6 +1828,7 @@ struct EngineKernel {
         rs.chunks = pend;
         n->middle_count = 0;
         n->active_count = 0;
+        n->popped = 0;
         // the previous round's deferred set ran at the start of this round; this
         // round's set either ran inside the round or is now pending
         n->heavy_count[cur ^ 1u] = 0;
@@ -1403,6 +1887,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
         a.qflag[1][w] = 0;
         a.qflag[2][w] = 0;
     }
+    if (a.tile_row) K::compute_tile_rows(a);
     if (!grid_sync(c, tmo, nop)) return false;
     K::rebuild(app, a, 0, acc);
     K::flush_acc(a, acc, 0, 2);
@@ -1487,7 +1972,9 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
                 const bool reduce_td = reduce && !dd && lb_pull != LB_NONE;  // scans every vertex, no middle list
                 K::combine_all(app, a, sync, !reduce_td);
                 if (!grid_sync(c, tmo, nop)) return false;
-                if (reduce_td) {
+                if (reduce_td && a.tile_row) {
+                    K::pull_tiles(app, a, my_lb, acc);
+                } else if (reduce_td) {
                     K::pull_reduce_td(app, a, s, my_lb, acc);
                     K::flush_acc(a, acc, s.qhi, s.qlo);
                     if (!grid_sync(c, tmo, nop)) return false;

@@ -54,7 +54,7 @@ constexpr uint32_t kWords = kNoAllocMaxVertices / 32 + 1;
 constexpr uint32_t kHeavyCap = (kNoAllocMaxVertices < kNoAllocMaxEdges / kHeavyDegree ? kNoAllocMaxVertices
                                                                                       : kNoAllocMaxEdges / kHeavyDegree) +
                                2;
-constexpr uint32_t kChunkCap = kNoAllocMaxEdges / kChunkEdges + kHeavyCap + 2;
+constexpr uint32_t kChunkCap = kNoAllocMaxEdges / kChunkEdges + 2 * kHeavyCap + 2;
 
 // Byte offsets of the regions inside the scratch array.
 constexpr size_t kOffBuffer = 0;
@@ -181,6 +181,7 @@ extern "C" sg_status sg_bfs_noalloc(const uint32_t *offsets, const uint32_t *ind
     p.pull_warp_threshold = 32;
     p.local_depth = o.local_depth > 0 ? (uint32_t)o.local_depth : 0u;
     p.sample_cut = 0.f;
+    p.bitmap_frontier = engine::use_bitmap_frontier(p.forced, p.lb_push, false, o.worklist);
     p.alpha = o.alpha;
     p.beta = o.beta > 0 ? o.beta : 18;
     p.total_workload0 = (long long)((double)ne * (o.edge_factor > 0 ? o.edge_factor : 1.0));

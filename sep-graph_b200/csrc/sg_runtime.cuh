@@ -188,6 +188,7 @@ struct EngineConfig {
     uint32_t local_depth = 0;  // local lookahead levels in push rounds (0 = off)
     float sample_cut = 0.f;    // sampling priority cut in ASYNC_PUSH_TD rounds (0 = off)
     bool wl_sort = false;      // sort each data-driven push round's worklist by vertex id (--wl_sort)
+    int worklist = 0;          // SG_WORKLIST_* (forced push DD: queues or bitmaps)
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -281,9 +282,12 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     // tables, one per round parity (a push round's chunks may run at the start
     // of the next round while that round registers its own).
     const uint32_t heavy_threshold = std::max<uint32_t>(1, cfg.heavy_degree);
-    const uint32_t chunk_edges = std::max<uint32_t>(32, cfg.chunk_edges);
+    // a multiple of 4: chunks start on 16-byte boundaries of the edge arrays
+    const uint32_t chunk_edges = (std::max<uint32_t>(32, cfg.chunk_edges) + 3u) & ~3u;
     const uint32_t heavy_cap = (uint32_t)std::min<uint64_t>(nv, ne / heavy_threshold) + 2;
-    const uint32_t chunk_cap = (uint32_t)(ne / chunk_edges + heavy_cap + 2);
+    // chunks are cut on the 4-edge grid (chunk_span): at most two more per
+    // heavy vertex than its degree / chunk_edges
+    const uint32_t chunk_cap = (uint32_t)(ne / chunk_edges + 2ull * heavy_cap + 2);
     auto &ws = sgb::graph_ws(g);
     SG_TRY_CUDA(ctx, ws.get("tmp", nv, &a.tmp));
     SG_TRY_CUDA(ctx, ws.get("q0", nv, &a.queue[0]));
@@ -320,6 +324,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     p.pull_warp_threshold = 32;
     p.local_depth = cfg.local_depth;
     p.sample_cut = cfg.sample_cut;
+    p.bitmap_frontier = use_bitmap_frontier(cfg.forced, cfg.lb_push, cfg.wl_sort, cfg.worklist);
     p.alpha = cfg.alpha;
     p.beta = cfg.beta;
     p.total_workload0 = (long long)((double)ne * cfg.edge_factor);
@@ -344,6 +349,13 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     dim3 grid(ctx->prop.multiProcessorCount * bps), block(kBlockThreads);
     res->grid_blocks = grid.x;
     if (cfg.wl_sort) SG_TRY_CUDA(ctx, ws.get("sort", grid.x, &a.sort_counts));
+    // edge-tiled topology-driven pull (functors with PullReduce): a row index per
+    // 256 in-edges, found once at the launch's start
+    if constexpr (has_pull_reduce<App, TB>::value && std::is_same<TW, sepgraph::graphs::NoWeight>::value) {
+        const bool td_pull = cfg.forced < 0 || cfg.forced == V_SYNC_PULL_TD;
+        if (g->has_csc && td_pull && cfg.lb_pull != LB_NONE && nv > 0)
+            SG_TRY_CUDA(ctx, ws.get("pull_tiles", (ne + kPullTileEdges - 1) / kPullTileEdges + 1, &a.tile_row));
+    }
 
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));

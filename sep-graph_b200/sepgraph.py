@@ -57,7 +57,7 @@ class Options(C.Structure):
         ("block_size", C.c_int32), ("non_atomic", C.c_int32), ("trace", C.c_int32), ("pr_error", C.c_double),
         ("timeout_s", C.c_double), ("blocking", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("heavy_degree", C.c_int32), ("chunk_edges", C.c_int32), ("team_blocks", C.c_int32),
-        ("local_depth", C.c_int32), ("wl_sort", C.c_int32), ("reserved", C.c_int32 * 1),
+        ("local_depth", C.c_int32), ("wl_sort", C.c_int32), ("worklist", C.c_int32),
     ]
 
 

@@ -113,6 +113,9 @@ def test_bfs_rmat(ctx, scale, sym):
         for variant in ("auto", "async_push_dd", "async_pull_dd"):
             lv, st, _ = G.bfs(int(src), variant=variant)
             assert (lv == ref).all(), (variant, src)
+        for kw in (dict(worklist=2), dict(worklist=2, non_atomic=0, local_depth=8)):
+            lv, st, _ = G.bfs(int(src), variant="async_push_dd", **kw)
+            assert (lv == ref).all(), (kw, src)
         assert st.edges_reached == np.diff(h.offsets)[ref != sg.INF].sum()
 
 
@@ -123,7 +126,10 @@ def test_sssp_rmat(ctx, scale):
     for src in h.pick_sources(4, 3):
         ref = oracle.sssp(h.offsets, h.indices, h.weights, int(src))
         for kw in (dict(), dict(variant="async_push_dd"), dict(priority="low_high"),
-                   dict(priority="low_high", priority_delta=8), dict(variant="async_pull_dd")):
+                   dict(priority="low_high", priority_delta=8), dict(variant="async_pull_dd"),
+                   dict(variant="async_push_dd", worklist=2),
+                   dict(variant="async_push_dd", priority="low_high", priority_delta=4, worklist=2, local_depth=16),
+                   dict(variant="async_push_dd", priority="low_high", priority_delta=8, worklist=1, chunk_edges=37)):
             d, st, _ = G.sssp(int(src), max_iteration=100000, **kw)
             assert (d == ref).all(), kw
 
@@ -187,6 +193,24 @@ def test_wl_sort_golden(ctx, path):
     for kw in (dict(variant="async_push_dd"), dict(priority="low_high")):
         d, _, _ = G.sssp(src, wl_sort=1, max_iteration=100000, **kw)
         assert (d == g["sssp"]).all(), kw
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
+def test_bitmap_worklists_golden(ctx, path):
+    """Bitmap worklists (sg_options.worklist = SG_WORKLIST_BITMAP) on the small
+    fixtures: BFS and SSSP with and without two-level priority and lookahead."""
+    g = _load(path)
+    G = _graph(ctx, g)
+    src = int(g["source"])
+    for kw in (dict(), dict(non_atomic=0, local_depth=4), dict(blocks_per_sm=8)):
+        lv, _, _ = G.bfs(src, variant="async_push_dd", worklist=2, **kw)
+        assert (lv == g["bfs"]).all(), kw
+    for kw in (dict(), dict(priority="low_high"), dict(priority="low_high", priority_delta=3, local_depth=8),
+               dict(chunk_edges=32, heavy_degree=1)):
+        d, _, _ = G.sssp(src, variant="async_push_dd", worklist=2, max_iteration=100000, **kw)
+        assert (d == g["sssp"]).all(), kw
+    r, _, _ = G.pagerank(variant="async_push_dd", worklist=2, pr_error=1e-7, max_iteration=100000)
+    assert _pr_l1(r, oracle.pagerank_f64(g["offsets"], g["indices"], 1e-12)) <= PR_L1_TOL
 
 
 @pytest.mark.parametrize("bps", [1, 8])
