@@ -630,10 +630,19 @@ def per_algo(ctx, cache, a):
     res["pagerank_rmat23"] = pr
     del hs
 
-    # BC RMAT-23 symmetrised, source = max-degree vertex
+    # BFS and BC on RMAT-23 symmetrised, source = max-degree vertex
     h = sg.HostGraph.rmat(23, 16, symmetric=True, seed=1)
     G = ctx.graph(h, symmetric=True)
     src = h.max_degree_vertex()[0]
+    t, (lv, st, _) = _median_ms(lambda: G.bfs(src), 6)
+    t0 = time.perf_counter()
+    ok = bool(np.array_equal(lv, oracle.bfs(h.offsets, h.indices, src)))
+    cpu_s = time.perf_counter() - t0
+    res["bfs_rmat23_sym"] = dict(
+        GTEPS=st.edges_reached / t / 1e6, GTEPS_graph500_half_edges=st.edges_reached / 2 / t / 1e6, ms=t,
+        rounds=st.rounds, rounds_by_variant=list(st.rounds_by_variant), edges_processed=st.edges_processed,
+        parity_vs_oracle=ok, **_roof(bfs_bytes(h.nv, st.edges_reached), t, peak),
+        cpu_GTEPS=st.edges_reached / cpu_s / 1e9, cpu_ms=1e3 * cpu_s, cpu="oracle BFSHost restatement, 1 thread")
     t, (bc, sig, st) = _median_ms(lambda: G.bc(src), 6, si=2, key="time_total_ms")
     e_r = st.edges_reached // 2  # sg_bc counts both traversals
     b = 2 * (4 * (h.nv + 1) + 4 * e_r) + 32 * h.nv

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SG_ABI_VERSION 1
+#define SG_ABI_VERSION 2
 
 typedef enum sg_status {
     SG_OK = 0,
@@ -104,6 +104,13 @@ typedef struct sg_options {
     int32_t worklist;         /* worklists of a forced SG_ASYNC_PUSH_DD run with load balancing: 0 = library
                                  choice, SG_WORKLIST_QUEUE = deduplicated queues, SG_WORKLIST_BITMAP = the
                                  output slot's bitmap itself (fire-and-forget bit sets, no appends) */
+    int32_t l2_persist;       /* L2 persistence window on the array a launch updates at random (the tentative
+                                 values; the pulled values of a topology-driven pull) for single-query
+                                 calls: 0 = library choice (on where the device supports it), 1 = on,
+                                 -1 = off.  Set on the launch's stream for that launch only; the L2
+                                 set-aside it needs is returned when the last context of the device is
+                                 destroyed. */
+    int32_t reserved[3];
 } sg_options;
 #define SG_WORKLIST_AUTO 0
 #define SG_WORKLIST_QUEUE 1

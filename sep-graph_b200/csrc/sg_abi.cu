@@ -131,6 +131,7 @@ sgb::EngineConfig make_config(const sg_graph *g, const sg_options &o, int scheme
     if (o.local_depth > 0) c.local_depth = (uint32_t)o.local_depth;
     c.wl_sort = o.wl_sort != 0;
     c.worklist = o.worklist;
+    c.l2_persist = o.l2_persist;
     // SetSampleBasedPriority (common.h:229-233; hybrid_pr.cu:135-137 sets it when --cut_threshold > 0)
     if (o.priority == SG_PRIORITY_SAMPLING && o.cut_threshold > 0) c.sample_cut = (float)std::min(o.cut_threshold, 1.0);
     c.blocking = o.blocking != 0;
@@ -239,6 +240,7 @@ sg_status sg_destroy(sg_ctx *ctx) {
         return set_error(ctx, SG_ERR_BUSY, "%d graph(s) of this context still exist", ctx->live_graphs);
     DeviceGuard dg(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    sgb::persist_release(ctx);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->spare_arena) cudaFree(ctx->spare_arena);
     delete ctx->batch_ws;

@@ -111,6 +111,10 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *queue, uint32_t *count
 __device__ __forceinline__ bool bitmap_test(const uint32_t *bm, uint32_t v) {
     return (ld_l2(bm + (v >> 5)) >> (v & 31u)) & 1u;
 }
+// For a bitmap no block writes during the current phase (read through L1).
+__device__ __forceinline__ bool bitmap_test_l1(const uint32_t *bm, uint32_t v) {
+    return (ld_l1(bm + (v >> 5)) >> (v & 31u)) & 1u;
+}
 // Returns true if this call set the bit.
 __device__ __forceinline__ bool bitmap_set(uint32_t *bm, uint32_t v) {
     const uint32_t bit = 1u << (v & 31u);

@@ -1309,6 +1309,69 @@ struct EngineKernel {
         return hit;
     }
 
+    // Warp-cooperative data-driven pull into up to 32 destinations of at most
+    // pull_warp_threshold in-edges each (one per lane; deg 0 = none): the warp
+    // walks their concatenated in-edge lists 32 edges at a time, so one
+    // coalesced load of sources and one batch of frontier-bit tests cover
+    // several destinations at once.  Per destination the frontier sources are
+    // taken in edge order, as the serial scan takes them (async_pull_dd.cuh:
+    // 34-136): the lowest pending lane of each destination calls
+    // AccumulateBuffer, a BREAK retires the destination (no further calls,
+    // later batches skip its edges), otherwise its next frontier source
+    // follows.  Returns whether some call succeeded for the lane's own
+    // destination.  All 32 lanes must call.
+    static __device__ bool pull_coop(App &app, const Args &a, const Snap &s, WarpLB<TB> &w, uint32_t v,
+                                     uint32_t beg, uint32_t deg, bool sync, Acc &acc) {
+        const uint32_t lane = dev::lane_id();
+        const TB *srcbuf = sync ? a.tmp : a.buffer;
+        const uint32_t *bin = a.bitmap[s.bin];
+        const uint32_t incl = dev::warp_inclusive_scan(deg);
+        const uint32_t total = __shfl_sync(dev::kFullMask, incl, 31);
+        if (total == 0) return false;
+        w.excl[lane] = incl - deg;
+        w.beg[lane] = beg;
+        w.src[lane] = v;
+        __syncwarp();
+        const uint32_t has = __ballot_sync(dev::kFullMask, deg > 0);
+        uint32_t done = 0, hitm = 0, scanned = 0;
+        for (uint32_t eb = 0; eb < total; eb += 32) {
+            const uint32_t e = eb + lane;
+            const bool valid = e < total;
+            const uint32_t k = valid ? owner(w.excl, e) : 0u;
+            const bool live = valid && !((done >> k) & 1u);
+            bool cand = false;
+            uint32_t u = 0, edge = 0;
+            if (live) {
+                edge = w.beg[k] + (e - w.excl[k]);
+                u = a.csc.edge_src(edge);
+                cand = dev::bitmap_test_l1(bin, u);  // the input frontier is read-only this round
+            }
+            scanned += __popc(__ballot_sync(dev::kFullMask, live));
+            // first lane of this lane's destination inside the batch
+            const uint32_t first = valid ? (w.excl[k] > eb ? w.excl[k] - eb : 0u) : lane;
+            const uint32_t below = ((1u << lane) - 1u) & ~((1u << first) - 1u);
+            uint32_t P = __ballot_sync(dev::kFullMask, cand);
+            while (P) {
+                const bool elected = ((P >> lane) & 1u) && !(P & below);
+                bool ok = false, brk = false;
+                if (elected) {
+                    const uint32_t dst = w.src[k];
+                    const int st =
+                        accumulate<App, TB, TW>(app, a.csc_w, u, dst, edge, a.buffer + dst, dev::ld_l2(srcbuf + u));
+                    ok = acc_success(st);
+                    brk = !acc_continue(st);
+                }
+                hitm |= __reduce_or_sync(dev::kFullMask, ok ? (1u << k) : 0u);
+                done |= __reduce_or_sync(dev::kFullMask, brk ? (1u << k) : 0u);
+                P &= ~__ballot_sync(dev::kFullMask, elected || (valid && ((done >> k) & 1u)));
+            }
+            if ((done & has) == has) break;  // every destination retired
+        }
+        if (lane == 0) acc.edges += scanned;
+        __syncwarp();
+        return (hitm >> lane) & 1u;
+    }
+
     // The whole warp pulls into one high in-degree destination, 32 in-edges per step.
     static __device__ bool pull_warp(App &app, const Args &a, const Snap &s, uint32_t v, uint32_t beg, uint32_t deg,
                                      bool dd, bool sync, Acc &acc) {
@@ -1336,8 +1399,8 @@ struct EngineKernel {
         return __any_sync(dev::kFullMask, hit);
     }
 
-    static __device__ void pull_phase(App &app, const Args &a, const Snap &s, bool dd, bool sync, int lb,
-                                      Acc &acc) {
+    static __device__ void pull_phase(App &app, const Args &a, const Snap &s, WarpLB<TB> &wlb, bool dd, bool sync,
+                                      int lb, Acc &acc) {
         const uint32_t lane = dev::lane_id();
         const uint32_t M = min(dev::ld_l2(&a.ctrl->cnt.middle_count), a.csr.nnodes);
         const bool natural = (M == a.csr.nnodes);  // every vertex scheduled: keep CSC order
@@ -1353,7 +1416,10 @@ struct EngineKernel {
             }
             const bool big = valid && lb != LB_NONE && deg > a.p.pull_warp_threshold;
             bool hit = false;
-            if (valid && !big) hit = pull_serial(app, a, s, v, beg, deg, dd, sync, acc);
+            if (dd && lb != LB_NONE)
+                hit = pull_coop(app, a, s, wlb, v, beg, valid && !big ? deg : 0u, sync, acc);
+            else if (valid && !big)
+                hit = pull_serial(app, a, s, v, beg, deg, dd, sync, acc);
             uint32_t bigmask = __ballot_sync(dev::kFullMask, big);
             while (bigmask) {
                 const uint32_t j = __ffs(bigmask) - 1;
@@ -1980,7 +2046,7 @@ __device__ bool run_instance(const App &app_in, const KArgs<TV, TB, TW> &a) {
                     if (!grid_sync(c, tmo, nop)) return false;
                     K::pull_reduce_chunks(app, a, set, acc);
                 } else {
-                    K::pull_phase(app, a, s, dd, sync, lb_pull, acc);
+                    K::pull_phase(app, a, s, my_lb, dd, sync, lb_pull, acc);
                 }
                 K::flush_acc(a, acc, s.qhi, s.qlo);
                 if (!dd) {

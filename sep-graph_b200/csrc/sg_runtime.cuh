@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -41,6 +42,7 @@ struct sg_ctx {
     // (between half its size and its size): reloading a graph costs no cudaMalloc/cudaFree
     void *spare_arena = nullptr;
     size_t spare_bytes = 0;
+    bool persist_ref = false;  // holds a reference on the device's persisting-L2 set-aside
 };
 
 namespace sgb {
@@ -189,6 +191,7 @@ struct EngineConfig {
     float sample_cut = 0.f;    // sampling priority cut in ASYNC_PUSH_TD rounds (0 = off)
     bool wl_sort = false;      // sort each data-driven push round's worklist by vertex id (--wl_sort)
     int worklist = 0;          // SG_WORKLIST_* (forced push DD: queues or bitmaps)
+    int l2_persist = 0;        // sg_options.l2_persist: >= 0 = persistence window on the random-access array
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -199,6 +202,95 @@ struct EngineResult {
     float ms = 0.f;
     uint32_t grid_blocks = 0;
     uint32_t device_error() const { return ctrl.error | ctrl.cnt.error; }
+};
+
+// ---------------------------------------------------------------- L2 persistence
+// The persisting-L2 set-aside of a device (cudaLimitPersistingL2CacheSize) is
+// raised to the device's maximum by the first context that launches with a
+// persistence window and put back, with the persisting lines reset to normal,
+// when the last such context of the device is destroyed.
+struct PersistState {
+    std::mutex mu;
+    int users = 0;
+    bool changed = false;
+    size_t prev = 0;
+};
+inline PersistState &persist_state(int dev) {
+    static PersistState st[64];
+    return st[dev & 63];
+}
+inline void persist_acquire(sg_ctx *ctx) {
+    if (ctx->persist_ref || ctx->prop.persistingL2CacheMaxSize <= 0 || ctx->prop.accessPolicyMaxWindowSize <= 0) return;
+    PersistState &st = persist_state(ctx->device);
+    std::lock_guard<std::mutex> lk(st.mu);
+    if (st.users == 0) {
+        size_t cur = 0;
+        if (cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        const size_t want = (size_t)ctx->prop.persistingL2CacheMaxSize;
+        if (cur < want) {
+            if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+                cudaGetLastError();
+                return;
+            }
+            st.changed = true;
+            st.prev = cur;
+        }
+    }
+    st.users++;
+    ctx->persist_ref = true;
+}
+inline void persist_release(sg_ctx *ctx) {
+    if (!ctx->persist_ref) return;
+    PersistState &st = persist_state(ctx->device);
+    std::lock_guard<std::mutex> lk(st.mu);
+    if (--st.users == 0 && st.changed) {
+        cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, st.prev);
+        cudaGetLastError();
+        st.changed = false;
+    }
+    ctx->persist_ref = false;
+}
+// Access-policy window for the launches made while it lives: `bytes` from
+// `base` marked persisting (as far as the set-aside reaches), then the
+// stream's previous window restored.
+struct PersistWindow {
+    cudaStream_t s = nullptr;
+    cudaStreamAttrValue old{};
+    bool set = false;
+    PersistWindow(sg_ctx *ctx, const void *base, size_t bytes) {
+        if (!ctx->persist_ref || !base || bytes == 0) return;
+        if (cudaStreamGetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &old) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        size_t lim = 0;
+        if (cudaDeviceGetLimit(&lim, cudaLimitPersistingL2CacheSize) != cudaSuccess || lim == 0) {
+            cudaGetLastError();
+            return;
+        }
+        cudaStreamAttrValue v{};
+        v.accessPolicyWindow.base_ptr = const_cast<void *>(base);
+        v.accessPolicyWindow.num_bytes = std::min(bytes, (size_t)ctx->prop.accessPolicyMaxWindowSize);
+        v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)lim / (double)v.accessPolicyWindow.num_bytes);
+        v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        if (cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        s = ctx->stream;
+        set = true;
+    }
+    ~PersistWindow() {
+        if (set && cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &old) != cudaSuccess)
+            cudaGetLastError();
+    }
+    PersistWindow(const PersistWindow &) = delete;
+    PersistWindow &operator=(const PersistWindow &) = delete;
 };
 
 // Resident blocks per SM of `kernel` at `threads` threads per block, computed
@@ -360,7 +452,15 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     void *args[] = {(void *)&app, (void *)&a};
-    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)kernel, grid, block, args, 0, ctx->stream));
+    {
+        // the array the rounds touch at random stays in L2 while the graph arrays stream past it:
+        // the pulled values of a topology-driven pull, the tentative values otherwise
+        if (cfg.l2_persist >= 0) persist_acquire(ctx);
+        const bool td_pull = cfg.forced == V_SYNC_PULL_TD && a.tile_row;
+        PersistWindow pw(ctx, td_pull ? (const void *)a.tmp : (const void *)a.buffer,
+                         cfg.l2_persist >= 0 ? sizeof(TB) * (size_t)nv : 0);
+        SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)kernel, grid, block, args, 0, ctx->stream));
+    }
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     if (!cfg.blocking) return SG_OK;
 
@@ -458,16 +558,19 @@ class Engine {
         m_status = sgb::run_engine<AppImpl, TValue, TBuffer, TWeight>(m_graph, *m_app, cfg, m_value, m_buffer, &m_res);
         return m_status;
     }
+    // GatherValue / GatherBuffer (framework.cuh:385-391): copied on the engine's
+    // stream (the graph's context stream), after the launch it ordered.
     const std::vector<TValue> &GatherValue() {
         m_value_host.resize(m_graph->nv);
-        cudaMemcpy(m_value_host.data(), m_value, sizeof(TValue) * m_graph->nv, cudaMemcpyDeviceToHost);
+        gather(m_value_host.data(), m_value, sizeof(TValue));
         return m_value_host;
     }
     const std::vector<TBuffer> &GatherBuffer() {
         m_buffer_host.resize(m_graph->nv);
-        cudaMemcpy(m_buffer_host.data(), m_buffer, sizeof(TBuffer) * m_graph->nv, cudaMemcpyDeviceToHost);
+        gather(m_buffer_host.data(), m_buffer, sizeof(TBuffer));
         return m_buffer_host;
     }
+    cudaStream_t getStream() const { return m_graph ? m_graph->ctx->stream : nullptr; }
     void PrintInfo() const {
         std::printf("Kernel time: %f\nTotal rounds: %u\n", m_res.ms, m_res.ctrl.round);
         for (int v = 0; v < 8; ++v)
@@ -476,6 +579,15 @@ class Engine {
                             m_res.ctrl.rounds_by_variant[v]);
     }
     const sgb::EngineResult &Result() const { return m_res; }
+
+   private:
+    void gather(void *dst, const void *src, size_t elem) {
+        if (!m_graph || !src) return;
+        cudaStream_t s = m_graph->ctx->stream;
+        if (cudaMemcpyAsync(dst, src, elem * m_graph->nv, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            m_status = SG_ERR_CUDA;
+    }
 };
 
 }  // namespace engine
