@@ -62,10 +62,11 @@ def args_parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--quick", action="store_true", help="headline line only")
-    p.add_argument("--served-queries", type=int, default=1000)
+    p.add_argument("--served-queries", type=int, default=2000)
     p.add_argument("--extras", default="per_algo,batched,ingest,served", help="extra sections at N=1 (comma list)")
     p.add_argument("--scale", type=int, default=SCALE)
-    p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc"],
+    p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc", "msbfs", "msbc",
+                                         "sssp_batch", "transpose"],
                    help="run one warm-up and one measured solve of that kernel only (for ncu captures)")
     p.add_argument("--opts", default="", help="--profile: JSON object of sg_options fields overriding the mode's")
     return p.parse_args()
@@ -76,6 +77,10 @@ def run_profile(a):
     import sepgraph as sg
 
     ctx = sg.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    if a.profile in ("msbfs", "msbc", "sssp_batch", "transpose"):
+        run_profile_batch(a, ctx)
+        ctx.close()
+        return
     sym = a.profile in ("bfs", "bc")
     h = sg.HostGraph.rmat(a.scale, EDGE_FACTOR, 0.57, 0.19, 0.19, seed=1, symmetric=sym)
     if a.profile.startswith("sssp"):
@@ -102,6 +107,47 @@ def run_profile(a):
                           "edges_reached": st.edges_reached, "edges_processed": st.edges_processed}), flush=True)
     G.close()
     ctx.close()
+
+
+def run_profile_batch(a, ctx):
+    """Two runs of one batched / multi-source / graph-construction call (the second is the one to capture):
+    msbfs 64 sources and msbc 32 sources on the symmetric RMAT graph of --scale; sssp_batch 64 SSSP
+    queries over RMAT graphs of scales 12 .. --scale; transpose = sg_graph_create of the directed
+    weighted RMAT CSR of --scale from device arrays (validation and the CSC transpose)."""
+    import sepgraph as sg
+    import torch
+
+    for _ in range(2):
+        t0 = time.perf_counter()
+        if a.profile in ("msbfs", "msbc"):
+            if _ == 0:
+                h = sg.HostGraph.rmat(a.scale, EDGE_FACTOR, seed=1, symmetric=True)
+                G = ctx.graph(h, symmetric=True)
+            n = 64 if a.profile == "msbfs" else 32
+            srcs = [int(x) for x in h.pick_sources(n, 11)]
+            out = G.msbfs(srcs) if a.profile == "msbfs" else G.msbc(srcs)
+            ms = out[1].time_kernel_ms
+        elif a.profile == "sssp_batch":
+            if _ == 0:
+                graphs = []
+                for sc in range(12, a.scale + 1):
+                    hh = sg.HostGraph.rmat(sc, 16, seed=100 + sc).gen_weights(1, 64, 200 + sc)
+                    graphs.append((hh, ctx.graph(hh, no_csc=True)))
+                rng = random.Random(5)
+                queries = [(graphs[k % len(graphs)][1], rng.randrange(graphs[k % len(graphs)][0].nv))
+                           for k in range(64)]
+            _, st, _ = ctx.sssp_batch(queries, variant="async_push_dd", max_iteration=1000000)
+            ms = st.time_kernel_ms
+        else:
+            if _ == 0:
+                h = sg.HostGraph.rmat(a.scale, EDGE_FACTOR, seed=1).gen_weights(1, 64, 2)
+                dev = [torch.from_numpy(x.view(np.int32)).cuda() for x in (h.offsets, h.indices, h.weights)]
+            torch.cuda.synchronize()
+            gg = ctx.graph_from_csr(*dev, nv=h.nv, ne=h.ne)
+            torch.cuda.synchronize()
+            gg.close()
+            ms = 1e3 * (time.perf_counter() - t0)
+        print(json.dumps({"profile": a.profile, "scale": a.scale, "ms": ms}), flush=True)
 
 
 def peak_hbm():
@@ -512,8 +558,11 @@ def oracle_dijkstra(h, s):
 
 
 def read_traffic(mode):
-    """DRAM bytes per launch of the engine kernel from the committed ncu summary of the selected mode."""
-    name = "sssp_rmat21_delta_engine_kernel.md" if mode.startswith("delta") else "sssp_rmat22_push_dd_engine_kernel.md"
+    """DRAM bytes per launch of the engine kernel from the committed ncu summary of the full-size
+    headline launch (delta-stepping options); None for a mode it does not describe."""
+    if not mode.startswith("delta"):
+        return None
+    name = "sssp_rmat22_delta_engine_kernel_traffic.md"
     try:
         for line in open(os.path.join(ROOT, "profiles", name)):
             if line.startswith("dram_bytes_per_launch_full_size:"):
@@ -860,7 +909,9 @@ SERVED_MIX = (("bfs", 0.60), ("sssp", 0.25), ("pagerank", 0.10), ("bc", 0.05))
 
 
 def served(ctx, cache, a):
-    """Mixed query stream through the server vs the plain path on a sample of it."""
+    """Mixed query stream through the server: throughput when offered far above
+    capacity, latency percentiles at 25 / 50 / 90 % of that capacity, and the plain
+    one-query-per-launch path on a uniform sample of the stream (results compared)."""
     import sepgraph as sg
 
     specs = [("rmat", sc) for sc in range(14, 23)] + [("grid", n) for n in (1024, 1448, 2048, 2560, 2896, 3584, 4096)]
@@ -904,9 +955,10 @@ def served(ctx, cache, a):
         return sinks[key]
 
     outs = [out_for(i, al, g) for i, (al, g, _) in enumerate(queries)]
-    def stream(qs, rate, seed):
+
+    def stream(qs, rate, seed, **cfg):
         """Submits qs with Poisson arrivals at `rate` queries/s; returns statuses, wall seconds, server stats."""
-        srv = sg.Server(0, slots=3, max_batch=256)
+        srv = sg.Server(0, slots=3, max_batch=256, **cfg)
         try:
             for _, _, gg in graphs:
                 srv.add_graph(gg)
@@ -927,13 +979,20 @@ def served(ctx, cache, a):
         finally:
             srv.close()
 
-    rate = 2000.0  # offered load, queries/s (Poisson): far above capacity, measures throughput
+    rate = 5000.0  # offered load, queries/s (Poisson): far above capacity, measures throughput
     statuses, wall, st = stream(queries, rate, 23)
     failed = sum(1 for s_, _ in statuses if s_ != 0)
-    # latency below capacity: the first half of the stream offered at half the measured throughput
-    half = queries[: nq // 2]
-    rate_low = 0.5 * nq / wall
-    _, wall_low, st_low = stream(half, rate_low, 29)
+    capacity = nq / wall
+    # the same overload with batches that mix graphs (the other batching policy)
+    _, wall_mixed, _ = stream(queries, rate, 23, batch_graphs=2)
+    # latency below capacity: Poisson streams offered at 25 / 50 / 90 % of the measured
+    # throughput, each of about 12 s (at least 200 queries, at most the whole stream)
+    loads = {}
+    for f in (0.25, 0.5, 0.9):
+        n = int(min(nq, max(200, 12.0 * f * capacity)))
+        _, w, sl = stream(queries[:n], f * capacity, 29 + int(100 * f))
+        loads[f"{int(100 * f)}pct"] = {"queries": n, "offered_qps": f * capacity, "served_qps": n / w,
+                                       "p50_ms": sl["p50_ms"], "p99_ms": sl["p99_ms"], "p999_ms": sl["p999_ms"]}
 
     # plain path: the sampled queries one at a time, results to host like the server's
     plain_lat, same, plain_failed, failed_plain = [], True, 0, set()
@@ -983,10 +1042,12 @@ def served(ctx, cache, a):
     served_qps = nq / wall
     return {
         "queries": nq, "offered_qps": rate, "mix": dict(SERVED_MIX), "graphs": [n for n, _, _ in graphs],
-        "below_capacity": {"queries": len(half), "offered_qps": rate_low, "served_qps": len(half) / wall_low,
-                           "p50_ms": st_low["p50_ms"], "p99_ms": st_low["p99_ms"], "p999_ms": st_low["p999_ms"]},
+        "stream_note": f"{nq} queries of the 100k-query configuration (same mix, graphs and arrival process); "
+                       f"the full 100k would take about {100000 / served_qps / 60:.0f} minutes at this rate",
         "served_qps": served_qps, "server_qps_first_to_last": st["qps"], "p50_ms": st["p50_ms"],
         "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "batches": st["batches"],
+        "load_points": loads, "batch_graphs": "one graph per batch (default)",
+        "mixed_graph_batches_qps": nq / wall_mixed,
         "failed": failed, "plain_failed": plain_failed, "hbm_peak_bytes": st["hbm_peak"],
         "hbm_budget_bytes": st["hbm_budget"], "sssp": "two-level priority, each graph's delta heuristic",
         "plain_sample": len(plain_lat), "plain_qps": plain_qps, "plain_p50_ms": pct(plain_lat_sorted, 0.5),

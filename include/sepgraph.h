@@ -303,8 +303,14 @@ typedef struct sg_server_config {
     uint32_t sssp_delta;       /* SSSP two-level priority delta; 0 = each graph's 32*avg_w/avg_deg */
     uint32_t pad;
     double pr_error;           /* PageRank residual threshold (default 1e-7) */
-    int32_t reserved[8];
+    int32_t batch_graphs;      /* 0 = library choice (SG_BATCH_ONE_GRAPH); SG_BATCH_ONE_GRAPH: a batch takes
+                                  the oldest query's peers of the same algorithm on the same graph, so a
+                                  query on a small graph never waits for a large graph's traversal;
+                                  SG_BATCH_MIXED: peers on any graph (one team batch across graphs) */
+    int32_t reserved[7];
 } sg_server_config;
+#define SG_BATCH_ONE_GRAPH 1
+#define SG_BATCH_MIXED 2
 typedef struct sg_query {
     int32_t algo;      /* SG_QUERY_* */
     uint32_t graph_id; /* from sg_server_add_graph */

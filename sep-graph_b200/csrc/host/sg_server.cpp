@@ -286,7 +286,10 @@ void sg_server::worker(int slot) {
             const int algo = pending.front().q.algo;
             const uint32_t graph = pending.front().q.graph_id;
             uint32_t cap = cfg.max_batch;
-            bool one_graph = algo == SG_QUERY_PAGERANK;
+            // one graph per batch (default): a batch lasts as long as its slowest
+            // query, so a query on a small graph batched with a large graph's
+            // traversal would wait for it
+            bool one_graph = algo == SG_QUERY_PAGERANK || cfg.batch_graphs != SG_BATCH_MIXED;
             if (algo == SG_QUERY_BFS) {
                 uint32_t same = 0;
                 for (auto &p : pending)

@@ -62,6 +62,30 @@ __device__ __forceinline__ T ld_l2(const T *p) {
 
 // 16-byte read-only load (ld.global.nc.v4); p must be 16-byte aligned.
 __device__ __forceinline__ uint4 ldg_v4(const uint32_t *p) { return __ldg(reinterpret_cast<const uint4 *>(p)); }
+
+// Streamed graph arrays (edge destinations, weights, in-edge sources) are read
+// with an L2 evict-first cache policy: a traversal streams hundreds of MB of
+// them through L2 once, and without the hint they push out the vertex state
+// (tentative values, frontier bitmaps, pulled values) that every round reads
+// at random.
+__device__ __forceinline__ uint64_t stream_policy() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ uint32_t ldg_stream(const uint32_t *p, uint64_t pol) {
+    uint32_t r;
+    asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "l"(pol));
+    return r;
+}
+// 16-byte form; p must be 16-byte aligned.
+__device__ __forceinline__ uint4 ldg_v4_stream(const uint32_t *p, uint64_t pol) {
+    uint4 r;
+    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(p), "l"(pol));
+    return r;
+}
 // Load through L1 of data written earlier in the same launch by other blocks:
 // valid after a grid barrier, whose acquire (thread 0) and __syncthreads order
 // this SM's later loads after every block's earlier writes.

@@ -772,9 +772,10 @@ struct EngineKernel {
             const uint32_t edge = w.beg[k] + (e - w.excl[k]);
             r.src = w.src[k];
             r.pay = w.pay[k];
-            r.dst = a.csr.edge_dest(edge);
+            const uint64_t pol = dev::stream_policy();
+            r.dst = dev::ldg_stream(a.csr.edge_dst + edge, pol);
             if constexpr (!std::is_same<TW, graphs::NoWeight>::value)
-                if (a.csr_w) r.wt = __ldg(a.csr_w + edge);
+                if (a.csr_w) r.wt = dev::ldg_stream(a.csr_w + edge, pol);
             asm volatile("prefetch.global.L2 [%0];" ::"l"(a.buffer + r.dst));
         }
         return r;
@@ -882,6 +883,7 @@ struct EngineKernel {
             const uint32_t *wts = a.csr_w;
             const bool vec = (reinterpret_cast<uintptr_t>(col) & 15u) == 0 &&
                              (reinterpret_cast<uintptr_t>(wts) & 15u) == 0;
+            const uint64_t pol = dev::stream_policy();
             const uint32_t nw = nwarps();
             uint32_t ch = gwarp();
             uint32_t e_next = ch < C ? dev::ld_l2(own + ch) : 0xffffffffu;
@@ -898,10 +900,10 @@ struct EngineKernel {
                     const uint32_t base = w0 + lane * 8u;
                     uint32_t d[8], wt[8];
                     if (vec && base + 8u <= E) {
-                        const uint4 x = dev::ldg_v4(col + base), y = dev::ldg_v4(col + base + 4);
+                        const uint4 x = dev::ldg_v4_stream(col + base, pol), y = dev::ldg_v4_stream(col + base + 4, pol);
                         d[0] = x.x, d[1] = x.y, d[2] = x.z, d[3] = x.w, d[4] = y.x, d[5] = y.y, d[6] = y.z, d[7] = y.w;
                         if (wts) {
-                            const uint4 p = dev::ldg_v4(wts + base), q = dev::ldg_v4(wts + base + 4);
+                            const uint4 p = dev::ldg_v4_stream(wts + base, pol), q = dev::ldg_v4_stream(wts + base + 4, pol);
                             wt[0] = p.x, wt[1] = p.y, wt[2] = p.z, wt[3] = p.w, wt[4] = q.x, wt[5] = q.y, wt[6] = q.z,
                             wt[7] = q.w;
                         } else {
@@ -913,8 +915,8 @@ struct EngineKernel {
                         for (int j = 0; j < 8; ++j) {
                             const uint32_t i = base + j;
                             const bool in = i >= lo && i < hi;
-                            d[j] = in ? __ldg(col + i) : 0u;
-                            wt[j] = in && wts ? __ldg(wts + i) : 1u;
+                            d[j] = in ? dev::ldg_stream(col + i, pol) : 0u;
+                            wt[j] = in && wts ? dev::ldg_stream(wts + i, pol) : 1u;
                         }
                     }
                     TB cand[8], cur[8];
@@ -1343,7 +1345,7 @@ struct EngineKernel {
             uint32_t u = 0, edge = 0;
             if (live) {
                 edge = w.beg[k] + (e - w.excl[k]);
-                u = a.csc.edge_src(edge);
+                u = dev::ldg_stream(a.csc.edge_source + edge, dev::stream_policy());
                 cand = dev::bitmap_test_l1(bin, u);  // the input frontier is read-only this round
             }
             scanned += __popc(__ballot_sync(dev::kFullMask, live));
@@ -1571,17 +1573,18 @@ struct EngineKernel {
             const uint32_t *crow = a.csc.col_start;
             const uint32_t *srcs = a.csc.edge_source;
             const bool aligned = (reinterpret_cast<uintptr_t>(srcs) & 15u) == 0;
+            const uint64_t pol = dev::stream_policy();
             const TB *vals = a.tmp;
             const TB idn = app.PullIdentity();
             for (uint32_t t = gwarp(); t < T; t += nwarps()) {
                 const uint32_t e0 = t * kPullTileEdges + lane * 8u;
                 uint32_t s[8];
                 if (aligned && e0 + 8u <= E) {
-                    const uint4 x = dev::ldg_v4(srcs + e0), y = dev::ldg_v4(srcs + e0 + 4);
+                    const uint4 x = dev::ldg_v4_stream(srcs + e0, pol), y = dev::ldg_v4_stream(srcs + e0 + 4, pol);
                     s[0] = x.x, s[1] = x.y, s[2] = x.z, s[3] = x.w, s[4] = y.x, s[5] = y.y, s[6] = y.z, s[7] = y.w;
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) s[j] = e0 + j < E ? __ldg(srcs + e0 + j) : 0u;
+                    for (int j = 0; j < 8; ++j) s[j] = e0 + j < E ? dev::ldg_stream(srcs + e0 + j, pol) : 0u;
                 }
                 TB g[8];
 #pragma unroll

@@ -115,7 +115,8 @@ class BatchQuery(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("max_batch", C.c_uint32),
                 ("max_pending", C.c_uint32), ("msbfs_min", C.c_uint32), ("sssp_delta", C.c_uint32),
-                ("pad", C.c_uint32), ("pr_error", C.c_double), ("reserved", C.c_int32 * 8)]
+                ("pad", C.c_uint32), ("pr_error", C.c_double), ("batch_graphs", C.c_int32),
+                ("reserved", C.c_int32 * 7)]
 
 
 class Query(C.Structure):

@@ -61,9 +61,10 @@ def test_reached_edges_counts_out_degrees_of_reached_vertices():
 
 
 def test_traffic_comes_from_the_committed_summaries():
-    for mode in ("delta8", "push"):
-        t = bench.read_traffic(mode)
-        assert t is not None and t > 0, mode
+    # the headline's delta-stepping launch has a committed full-size capture; plain push has none
+    t = bench.read_traffic("delta8")
+    assert t is not None and t > 1e8
+    assert bench.read_traffic("push") is None
     peak, kind = bench.peak_hbm()
     assert peak > 0 and kind in ("measured", "fallback")
 
