@@ -988,11 +988,12 @@ def served(ctx, cache, a):
     # latency below capacity: Poisson streams offered at 25 / 50 / 90 % of the measured
     # throughput, each of about 12 s (at least 200 queries, at most the whole stream)
     loads = {}
-    for f in (0.25, 0.5, 0.9):
+    for f, order in ((0.25, 0), (0.5, 0), (0.9, 0), (0.5, 2)):
         n = int(min(nq, max(200, 12.0 * f * capacity)))
-        _, w, sl = stream(queries[:n], f * capacity, 29 + int(100 * f))
-        loads[f"{int(100 * f)}pct"] = {"queries": n, "offered_qps": f * capacity, "served_qps": n / w,
-                                       "p50_ms": sl["p50_ms"], "p99_ms": sl["p99_ms"], "p999_ms": sl["p999_ms"]}
+        _, w, sl = stream(queries[:n], f * capacity, 29 + int(100 * f), order=order)
+        key = f"{int(100 * f)}pct" + ("_oldest_first" if order == 2 else "")
+        loads[key] = {"queries": n, "offered_qps": f * capacity, "served_qps": n / w,
+                      "p50_ms": sl["p50_ms"], "p99_ms": sl["p99_ms"], "p999_ms": sl["p999_ms"]}
 
     # plain path: the sampled queries one at a time, results to host like the server's
     plain_lat, same, plain_failed, failed_plain = [], True, 0, set()
@@ -1047,6 +1048,8 @@ def served(ctx, cache, a):
         "served_qps": served_qps, "server_qps_first_to_last": st["qps"], "p50_ms": st["p50_ms"],
         "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "batches": st["batches"],
         "load_points": loads, "batch_graphs": "one graph per batch (default)",
+        "order": "shortest measured (algorithm, graph) batch first, 500 ms aging bound (default); "
+                 "one load point repeated oldest-first for comparison",
         "mixed_graph_batches_qps": nq / wall_mixed,
         "failed": failed, "plain_failed": plain_failed, "hbm_peak_bytes": st["hbm_peak"],
         "hbm_budget_bytes": st["hbm_budget"], "sssp": "two-level priority, each graph's delta heuristic",

@@ -285,11 +285,11 @@ sg_status sg_batch_plan_destroy(sg_batch_plan *plan);
 /* ------------------------------------------------------------------ serving
  * No counterpart in the reference.  A query server over device-resident
  * graphs with continuous batching: `slots` worker threads, each with its own
- * context and stream, repeatedly take the pending queries of one algorithm
- * (oldest first, up to max_batch), admit them against the HBM budget and run
- * them as one batched launch (multi-source BFS per graph, sg_sssp_batch /
- * sg_bfs_batch across graphs, one PageRank per graph shared by its queries,
- * sg_bc_batch).  Queries that arrive while batches run are taken as soon as
+ * context and stream, repeatedly take a group of pending queries (one
+ * algorithm on one graph by default, chosen by `order`, up to max_batch),
+ * admit them against the HBM budget and run them as one batched launch
+ * (multi-source BFS or BC per graph, sg_sssp_batch / sg_bfs_batch /
+ * sg_bc_batch teams, one PageRank per graph shared by its queries).  Queries that arrive while batches run are taken as soon as
  * a slot frees; batches of different slots overlap on the device.  Every
  * result equals the single-query call's. */
 typedef struct sg_server sg_server;
@@ -307,10 +307,18 @@ typedef struct sg_server_config {
                                   the oldest query's peers of the same algorithm on the same graph, so a
                                   query on a small graph never waits for a large graph's traversal;
                                   SG_BATCH_MIXED: peers on any graph (one team batch across graphs) */
-    int32_t reserved[7];
+    int32_t order;             /* which pending group a free slot takes: 0 = library choice
+                                  (SG_ORDER_SHORTEST_FIRST); SG_ORDER_SHORTEST_FIRST: the (algorithm, graph)
+                                  group whose batches have run shortest so far (measured per group, untried
+                                  groups first), unless the oldest query has waited longer than max_wait_ms,
+                                  whose group then goes first; SG_ORDER_OLDEST_FIRST: arrival order */
+    uint32_t max_wait_ms;      /* aging bound of SG_ORDER_SHORTEST_FIRST (0 = 500 ms) */
+    int32_t reserved[5];
 } sg_server_config;
 #define SG_BATCH_ONE_GRAPH 1
 #define SG_BATCH_MIXED 2
+#define SG_ORDER_SHORTEST_FIRST 1
+#define SG_ORDER_OLDEST_FIRST 2
 typedef struct sg_query {
     int32_t algo;      /* SG_QUERY_* */
     uint32_t graph_id; /* from sg_server_add_graph */

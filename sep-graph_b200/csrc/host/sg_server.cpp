@@ -2,7 +2,9 @@
 // (declarations and contract in include/sepgraph.h, "serving").
 //
 // Each slot is a worker thread with its own sg_ctx (stream, batch scratch).  A
-// free slot takes the pending queries of the oldest request's algorithm,
+// free slot picks a group of pending queries (by default one algorithm on one
+// graph, the group whose batches have run shortest so far, with an aging
+// bound that serves the oldest query's group first once it waited too long),
 // reserves an estimate of their device scratch against the HBM budget (waiting
 // for other slots to release memory when it does not fit), runs them as one
 // batched launch and completes their tickets.  Requests that arrive while a
@@ -75,6 +77,8 @@ struct sg_server {
     uint64_t budget = 0, in_use = 0, peak = 0;
     uint64_t submitted = 0, completed = 0, failed = 0, batches = 0;
     std::vector<double> latencies;
+    // measured batch time per (algorithm, graph) group, for shortest-first selection
+    std::map<std::pair<int, uint32_t>, double> group_ms;
     bool have_first = false;
     // optional batch log (one line per batch) when SEPGRAPH_SERVER_LOG names a file
     FILE *log = nullptr;
@@ -283,8 +287,30 @@ void sg_server::worker(int slot) {
             // that graph alone (up to 64 sources), and PageRank is one run per graph
             // for all its pending queries, so that other slots run the other graphs'
             // launches at the same time.
-            const int algo = pending.front().q.algo;
-            const uint32_t graph = pending.front().q.graph_id;
+            int algo = pending.front().q.algo;
+            uint32_t graph = pending.front().q.graph_id;
+            if (cfg.order != SG_ORDER_OLDEST_FIRST && cfg.batch_graphs != SG_BATCH_MIXED) {
+                // shortest expected batch first: the group whose batches have run
+                // shortest so far (a group never run yet counts as shortest, which
+                // also measures it), so a small query does not queue behind large
+                // graphs' traversals; a query older than max_wait_ms goes first
+                const double max_wait = cfg.max_wait_ms ? (double)cfg.max_wait_ms : 500.0;
+                const double waited =
+                    std::chrono::duration<double, std::milli>(Clock::now() - pending.front().t_submit).count();
+                if (waited <= max_wait) {
+                    double best = -1;
+                    for (auto &p : pending) {
+                        auto it = group_ms.find({p.q.algo, p.q.graph_id});
+                        const double c = it == group_ms.end() ? 0.0 : it->second;
+                        if (best < 0 || c < best) {
+                            best = c;
+                            algo = p.q.algo;
+                            graph = p.q.graph_id;
+                            if (c == 0.0) break;
+                        }
+                    }
+                }
+            }
             uint32_t cap = cfg.max_batch;
             // one graph per batch (default): a batch lasts as long as its slowest
             // query, so a query on a small graph batched with a large graph's
@@ -334,6 +360,12 @@ void sg_server::worker(int slot) {
         {
             std::lock_guard<std::mutex> lk(mu);
             in_use -= est;
+            {  // the group's batch time, smoothed over its batches
+                const double ms = std::chrono::duration<double, std::milli>(now - t_run).count();
+                const auto key = std::make_pair(batch.front().q.algo, batch.front().q.graph_id);
+                auto it = group_ms.find(key);
+                group_ms[key] = it == group_ms.end() ? ms : 0.7 * it->second + 0.3 * ms;
+            }
             for (size_t i = 0; i < batch.size(); ++i) {
                 TicketState &t = tickets[batch[i].ticket];
                 t.done = true;
