@@ -286,7 +286,7 @@ sg_status sg_batch_plan_destroy(sg_batch_plan *plan);
  * No counterpart in the reference.  A query server over device-resident
  * graphs with continuous batching: `slots` worker threads, each with its own
  * context and stream, repeatedly take a group of pending queries (one
- * algorithm on one graph by default, chosen by `order`, up to max_batch),
+ * algorithm, across graphs by default, up to max_batch),
  * admit them against the HBM budget and run them as one batched launch
  * (multi-source BFS or BC per graph, sg_sssp_batch / sg_bfs_batch /
  * sg_bc_batch teams, one PageRank per graph shared by its queries).  Queries that arrive while batches run are taken as soon as
@@ -303,15 +303,17 @@ typedef struct sg_server_config {
     uint32_t sssp_delta;       /* SSSP two-level priority delta; 0 = each graph's 32*avg_w/avg_deg */
     uint32_t pad;
     double pr_error;           /* PageRank residual threshold (default 1e-7) */
-    int32_t batch_graphs;      /* 0 = library choice (SG_BATCH_ONE_GRAPH); SG_BATCH_ONE_GRAPH: a batch takes
-                                  the oldest query's peers of the same algorithm on the same graph, so a
-                                  query on a small graph never waits for a large graph's traversal;
-                                  SG_BATCH_MIXED: peers on any graph (one team batch across graphs) */
-    int32_t order;             /* which pending group a free slot takes: 0 = library choice
-                                  (SG_ORDER_SHORTEST_FIRST); SG_ORDER_SHORTEST_FIRST: the (algorithm, graph)
-                                  group whose batches have run shortest so far (measured per group, untried
-                                  groups first), unless the oldest query has waited longer than max_wait_ms,
-                                  whose group then goes first; SG_ORDER_OLDEST_FIRST: arrival order */
+    int32_t batch_graphs;      /* 0 = library choice (SG_BATCH_MIXED); SG_BATCH_MIXED: a batch takes the
+                                  chosen query's peers of the same algorithm on any graph (one team batch
+                                  across graphs: the highest throughput); SG_BATCH_ONE_GRAPH: peers on the
+                                  same graph only, so a query on a small graph never waits for a large
+                                  graph's traversal inside its batch */
+    int32_t order;             /* with SG_BATCH_ONE_GRAPH, which pending group a free slot takes: 0 = library
+                                  choice (SG_ORDER_SHORTEST_FIRST); SG_ORDER_SHORTEST_FIRST: the (algorithm,
+                                  graph) group whose batches have run shortest so far (measured per group,
+                                  untried groups first), unless the oldest query has waited longer than
+                                  max_wait_ms, whose group then goes first; SG_ORDER_OLDEST_FIRST: the
+                                  oldest query's group.  Mixed batches always start from the oldest query. */
     uint32_t max_wait_ms;      /* aging bound of SG_ORDER_SHORTEST_FIRST (0 = 500 ms) */
     int32_t reserved[5];
 } sg_server_config;

@@ -2,9 +2,10 @@
 // (declarations and contract in include/sepgraph.h, "serving").
 //
 // Each slot is a worker thread with its own sg_ctx (stream, batch scratch).  A
-// free slot picks a group of pending queries (by default one algorithm on one
-// graph, the group whose batches have run shortest so far, with an aging
-// bound that serves the oldest query's group first once it waited too long),
+// free slot takes the pending queries of the oldest request's algorithm (or,
+// with one graph per batch, of the (algorithm, graph) group whose batches have
+// run shortest so far, with an aging bound that serves the oldest query's
+// group first once it waited too long),
 // reserves an estimate of their device scratch against the HBM budget (waiting
 // for other slots to release memory when it does not fit), runs them as one
 // batched launch and completes their tickets.  Requests that arrive while a
@@ -289,7 +290,8 @@ void sg_server::worker(int slot) {
             // launches at the same time.
             int algo = pending.front().q.algo;
             uint32_t graph = pending.front().q.graph_id;
-            if (cfg.order != SG_ORDER_OLDEST_FIRST && cfg.batch_graphs != SG_BATCH_MIXED) {
+            const bool one_graph_batches = cfg.batch_graphs == SG_BATCH_ONE_GRAPH;
+            if (one_graph_batches && cfg.order != SG_ORDER_OLDEST_FIRST) {
                 // shortest expected batch first: the group whose batches have run
                 // shortest so far (a group never run yet counts as shortest, which
                 // also measures it), so a small query does not queue behind large
@@ -312,10 +314,11 @@ void sg_server::worker(int slot) {
                 }
             }
             uint32_t cap = cfg.max_batch;
-            // one graph per batch (default): a batch lasts as long as its slowest
-            // query, so a query on a small graph batched with a large graph's
-            // traversal would wait for it
-            bool one_graph = algo == SG_QUERY_PAGERANK || cfg.batch_graphs != SG_BATCH_MIXED;
+            // one graph per batch (SG_BATCH_ONE_GRAPH): a batch lasts as long as its
+            // slowest query, so a query on a small graph batched with a large
+            // graph's traversal would wait for it; mixed batches (default) run
+            // more queries per launch
+            bool one_graph = algo == SG_QUERY_PAGERANK || one_graph_batches;
             if (algo == SG_QUERY_BFS) {
                 uint32_t same = 0;
                 for (auto &p : pending)

@@ -66,9 +66,11 @@ def _check(graphs, algo, gid, src, got):
         assert np.allclose(got, want, rtol=1e-4, atol=1e-5)
 
 
-def test_results_same_alone_and_in_the_mix(setup):
+@pytest.mark.parametrize("policy", [dict(), dict(batch_graphs=1), dict(batch_graphs=1, order=2)],
+                         ids=["mixed", "one_graph_shortest_first", "one_graph_oldest_first"])
+def test_results_same_alone_and_in_the_mix(setup, policy):
     ctx, graphs = setup
-    srv = sg.Server(0, slots=3, max_batch=64)
+    srv = sg.Server(0, slots=3, max_batch=64, **policy)
     try:
         gids = [srv.add_graph(G) for _, G in graphs]
         assert gids == list(range(len(graphs)))
