@@ -110,8 +110,13 @@ typedef struct sg_options {
                                  -1 = off.  Set on the launch's stream for that launch only; the L2
                                  set-aside it needs is returned when the last context of the device is
                                  destroyed. */
-    int32_t reserved[3];
+    int32_t pull_scan;        /* data-driven pull into vertices of at most 32 in-edges: 0 = library choice
+                                 (SG_PULL_SCAN_THREAD), SG_PULL_SCAN_THREAD = one thread per vertex with early
+                                 exit, SG_PULL_SCAN_WARP = a warp walks 32 vertices' in-edge lists together */
+    int32_t reserved[2];
 } sg_options;
+#define SG_PULL_SCAN_THREAD 1
+#define SG_PULL_SCAN_WARP 2
 #define SG_WORKLIST_AUTO 0
 #define SG_WORKLIST_QUEUE 1
 #define SG_WORKLIST_BITMAP 2

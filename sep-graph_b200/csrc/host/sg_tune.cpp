@@ -229,6 +229,12 @@ extern "C" sg_status sg_autotune(sg_graph *g, int algo, const uint32_t *sources,
             trial(c);
         }
     }
+    if (best->variant == SG_VARIANT_AUTO || best->variant == SG_ASYNC_PULL_DD) {
+        // the two forms of the data-driven pull into small in-degree vertices
+        sg_options c = *best;
+        c.pull_scan = best->pull_scan == SG_PULL_SCAN_WARP ? SG_PULL_SCAN_THREAD : SG_PULL_SCAN_WARP;
+        trial(c);
+    }
     if (best->variant == SG_ASYNC_PUSH_DD && best->lb_push != SG_LB_NONE && !best->wl_sort) {
         // the two worklist kinds of a forced data-driven push
         const sg_options cur = *best;

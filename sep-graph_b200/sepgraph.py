@@ -58,7 +58,7 @@ class Options(C.Structure):
         ("timeout_s", C.c_double), ("blocking", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("heavy_degree", C.c_int32), ("chunk_edges", C.c_int32), ("team_blocks", C.c_int32),
         ("local_depth", C.c_int32), ("wl_sort", C.c_int32), ("worklist", C.c_int32),
-        ("l2_persist", C.c_int32), ("reserved", C.c_int32 * 3),
+        ("l2_persist", C.c_int32), ("pull_scan", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -67,7 +67,7 @@ class TuneEntry(C.Structure):
 
 
 TUNED_FIELDS = ("variant", "blocks_per_sm", "heavy_degree", "chunk_edges", "priority", "priority_delta", "lb_push",
-                "local_depth", "worklist")
+                "local_depth", "worklist", "pull_scan")
 VARIANT_NAMES = {-1: "auto", 0: "sync_push_td", 1: "sync_push_dd", 2: "sync_pull_td", 3: "sync_pull_dd",
                  4: "async_push_td", 5: "async_push_dd", 6: "async_pull_td", 7: "async_pull_dd"}
 

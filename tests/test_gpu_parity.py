@@ -116,6 +116,9 @@ def test_bfs_rmat(ctx, scale, sym):
         for kw in (dict(worklist=2), dict(worklist=2, non_atomic=0, local_depth=8)):
             lv, st, _ = G.bfs(int(src), variant="async_push_dd", **kw)
             assert (lv == ref).all(), (kw, src)
+        for kw in (dict(pull_scan=2), dict(pull_scan=2, variant="async_pull_dd")):  # warp-cooperative pull
+            lv, st, _ = G.bfs(int(src), **kw)
+            assert (lv == ref).all(), (kw, src)
         assert st.edges_reached == np.diff(h.offsets)[ref != sg.INF].sum()
 
 
@@ -174,10 +177,11 @@ def test_bc_rmat(ctx):
     h = sg.HostGraph.rmat(14, 16, symmetric=True, seed=1)
     G = ctx.graph(h, symmetric=True)
     for src in [h.max_degree_vertex()[0], int(h.pick_sources(1, 3)[0])]:
-        bc, sigma, st = G.bc(int(src))
         bc64, sig64, _ = oracle.bc_f64(h.offsets, h.indices, int(src))
-        assert (sigma.astype(np.float64) == sig64).all()
-        assert np.allclose(bc, bc64, rtol=BC_RTOL, atol=BC_ATOL)
+        for kw in (dict(), dict(pull_scan=2), dict(pull_scan=2, variant="async_pull_dd")):
+            bc, sigma, st = G.bc(int(src), **kw)
+            assert (sigma.astype(np.float64) == sig64).all(), kw
+            assert np.allclose(bc, bc64, rtol=BC_RTOL, atol=BC_ATOL), kw
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
