@@ -113,7 +113,10 @@ typedef struct sg_options {
     int32_t pull_scan;        /* data-driven pull into vertices of at most 32 in-edges: 0 = library choice
                                  (SG_PULL_SCAN_THREAD), SG_PULL_SCAN_THREAD = one thread per vertex with early
                                  exit, SG_PULL_SCAN_WARP = a warp walks 32 vertices' in-edge lists together */
-    int32_t reserved[2];
+    int32_t hub_stage;        /* 256-edge hub chunks of SSSP: 0 = library choice, 1 = each chunk's
+                                 destinations and weights staged in shared memory by bulk copies (TMA engine)
+                                 one chunk ahead, -1 = read from global memory by each lane */
+    int32_t reserved[1];
 } sg_options;
 #define SG_PULL_SCAN_THREAD 1
 #define SG_PULL_SCAN_WARP 2

@@ -133,6 +133,7 @@ sgb::EngineConfig make_config(const sg_graph *g, const sg_options &o, int scheme
     c.worklist = o.worklist;
     c.l2_persist = o.l2_persist;
     c.pull_scan = o.pull_scan;
+    c.hub_stage = o.hub_stage;
     // SetSampleBasedPriority (common.h:229-233; hybrid_pr.cu:135-137 sets it when --cut_threshold > 0)
     if (o.priority == SG_PRIORITY_SAMPLING && o.cut_threshold > 0) c.sample_cut = (float)std::min(o.cut_threshold, 1.0);
     c.blocking = o.blocking != 0;

@@ -945,6 +945,7 @@ engine::Params batch_params(const sg_options &o, int scheme) {
     p.sample_cut = o.priority == SG_PRIORITY_SAMPLING && o.cut_threshold > 0 ? (float)std::min(o.cut_threshold, 1.0) : 0.f;
     p.bitmap_frontier = engine::use_bitmap_frontier(p.forced, p.lb_push, false, o.worklist);
     p.pull_coop = o.pull_scan == SG_PULL_SCAN_WARP;
+    p.stage_chunks = o.hub_stage >= 0;
     p.alpha = o.alpha;
     p.beta = o.beta > 0 ? o.beta : 18;
     p.timeout_ns = (unsigned long long)((o.timeout_s > 0 ? o.timeout_s : 30.0) * 1e9);

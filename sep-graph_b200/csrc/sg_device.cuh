@@ -86,6 +86,61 @@ __device__ __forceinline__ uint4 ldg_v4_stream(const uint32_t *p, uint64_t pol) 
         : "l"(p), "l"(pol));
     return r;
 }
+// ---- bulk copies (TMA engine, no tensor map) into shared memory, completed on
+// an mbarrier.  The source is always this GPU's own global memory and the
+// destination this CTA's own shared memory.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    // make the initialised barrier visible to the bulk-copy (async) proxy
+    asm volatile("fence.mbarrier_init.release.cluster;\n\tfence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long *bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// Orders this thread's earlier generic-proxy shared-memory accesses (reads of
+// a staging buffer) before bulk copies it issues next into that buffer.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// One arrival that also announces `bytes` of bulk-copy data for the phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// dst (shared) and src (global) 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the barrier's phase of the given parity to complete, giving up
+// after timeout_ns (false).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t parity,
+                                                  unsigned long long timeout_ns) {
+    uint64_t t0 = 0;
+    for (uint32_t n = 1;; ++n) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((n & 63u) == 0) {
+            const uint64_t t = globaltimer_ns();
+            if (t0 == 0)
+                t0 = t;
+            else if (t - t0 > timeout_ns)
+                return false;
+        }
+    }
+}
+
 // Load through L1 of data written earlier in the same launch by other blocks:
 // valid after a grid barrier, whose acquire (thread 0) and __syncthreads order
 // this SM's later loads after every block's earlier writes.

@@ -127,6 +127,8 @@ struct Params {
     // round takes its items from that bitmap (see push_phase_a).  The slot
     // counters then count pushes, not distinct vertices (zero iff empty).
     int32_t bitmap_frontier;
+    // Hub chunks of min-relax functors staged by bulk copies (256-edge chunks).
+    int32_t stage_chunks;
     // Data-driven pull into vertices of at most pull_warp_threshold in-edges:
     // 1 = a warp walks 32 vertices' in-edge lists together (pull_coop), 0 = a
     // thread per vertex with early exit (pull_serial).  Measured on B200 the
@@ -870,13 +872,52 @@ struct EngineKernel {
         }
     }
 
+    // The 8 edge slots [base, base + 8) of one window of a hub chunk, already in
+    // registers (d, wt), relaxed by one lane: the 8 current destination values
+    // are loaded together, the improving minima issued as reductions, the
+    // improved destinations pushed in one batch.  All 32 lanes must call.
+    static __device__ __forceinline__ void relax_slots(App &app, const Args &a, const Snap &s, uint32_t src,
+                                                       TB payload, uint32_t lo, uint32_t hi, uint32_t base,
+                                                       uint32_t (&d)[8], const uint32_t (&wt)[8], bool dd, Acc &acc) {
+        if constexpr (has_min_relax<App, TB, TW>::value) {
+            TB cand[8], cur[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t i = base + j;
+                const bool in = i >= lo && i < hi;
+                cand[j] = in ? app.RelaxCandidate(src, d[j], (TW)wt[j], payload) : std::numeric_limits<TB>::max();
+                cur[j] = in ? dev::ld_l2(a.buffer + d[j]) : (TB)0;
+            }
+            bool want[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                want[j] = cand[j] < cur[j];
+                if (want[j]) atomicMin(a.buffer + d[j], cand[j]);
+                want[j] = want[j] && dd;
+            }
+            enqueue_batch<8>(app, a, s, d, want, cand, acc, nullptr);
+        }
+    }
+
     // Hub chunks of a min-relax functor: lane l takes the 8 edge slots
-    // [w + 8l, w + 8l + 8) of each 256-slot window w of the chunk (two 16-byte
-    // loads each of destinations and weights; windows start on the chunk
-    // grid's 16-byte boundaries), loads the 8 current destination values
-    // together, issues the improving minima as reductions and pushes the
-    // improved destinations.  The next chunk's owner entry is loaded while
-    // the current chunk relaxes.
+    // [w + 8l, w + 8l + 8) of each 256-slot window w of the chunk (windows
+    // start on the chunk grid's 16-byte boundaries) and relaxes them with
+    // relax_slots.  With 256-edge chunks (one window each) and 16-byte aligned
+    // edge arrays, a chunk's destinations and weights are staged by the TMA
+    // engine: while the warp relaxes chunk k from registers, a bulk copy
+    // (cp.async.bulk, completed on the warp's mbarrier) brings chunk k+1's
+    // window into the warp's shared-memory stage, and lane 0 already fetches
+    // the descriptor of chunk k+2, so the adjacency's HBM latency overlaps
+    // the relaxations instead of preceding them.  Otherwise lanes load their
+    // slots with two 16-byte loads per array.
+    struct alignas(16) ChunkStage {
+        uint32_t dst[256];
+        uint32_t wt[256];
+        unsigned long long bar;
+        uint32_t src, lo, hi, w0, ncopy, pad;
+        TB pay;
+    };
+
     static __device__ void heavy_phase_relax(App &app, const Args &a, const Snap &s, uint32_t set, bool dd,
                                              Acc &acc) {
         if constexpr (has_min_relax<App, TB, TW>::value) {
@@ -893,6 +934,10 @@ struct EngineKernel {
                              (reinterpret_cast<uintptr_t>(wts) & 15u) == 0;
             const uint64_t pol = dev::stream_policy();
             const uint32_t nw = nwarps();
+            if (vec && ce == 256u && a.p.stage_chunks) {
+                heavy_phase_staged(app, a, s, dd, acc, C, H, own, items);
+                return;
+            }
             uint32_t ch = gwarp();
             uint32_t e_next = ch < C ? dev::ld_l2(own + ch) : 0xffffffffu;
             for (; ch < C; ch += nw) {
@@ -927,27 +972,120 @@ struct EngineKernel {
                             wt[j] = in && wts ? dev::ldg_stream(wts + i, pol) : 1u;
                         }
                     }
-                    TB cand[8], cur[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const uint32_t i = base + j;
-                        const bool in = i >= lo && i < hi;
-                        cand[j] = in ? app.RelaxCandidate(h.src, d[j], (TW)wt[j], h.payload)
-                                     : std::numeric_limits<TB>::max();
-                        cur[j] = in ? dev::ld_l2(a.buffer + d[j]) : (TB)0;
-                    }
-                    bool want[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        want[j] = cand[j] < cur[j];
-                        if (want[j]) atomicMin(a.buffer + d[j], cand[j]);
-                        want[j] = want[j] && dd;
-                    }
-                    enqueue_batch<8>(app, a, s, d, want, cand, acc, nullptr);
+                    relax_slots(app, a, s, h.src, h.payload, lo, hi, base, d, wt, dd, acc);
                 }
                 if (lane == 0) acc.edges += hi - lo;
             }
         }
+    }
+
+    // The staged form of heavy_phase_relax (256-edge chunks, aligned arrays).
+    static __device__ void heavy_phase_staged(App &app, const Args &a, const Snap &s, bool dd, Acc &acc,
+                                              uint32_t C, uint32_t H, const uint32_t *own,
+                                              const HeavyItem<TB> *items) {
+        __shared__ ChunkStage stage[kWarpsPerBlock];
+        ChunkStage &st = stage[dev::warp_id()];
+        const uint32_t lane = dev::lane_id();
+        const uint32_t E = a.csr.nedges;
+        const uint32_t *col = a.csr.edge_dst;
+        const uint32_t *wts = a.csr_w;
+        const uint32_t nw = nwarps();
+        uint32_t c = gwarp();
+        if (c >= C) return;
+        // Lane 0 only: stage chunk `ch` (descriptor h, from owner entry e) — the
+        // window's metadata, then one arrival announcing the copy's bytes and the
+        // bulk copies; a chunk with no edges completes the phase with 0 bytes.
+        auto issue = [&](uint32_t ch, uint32_t e, const HeavyItem<TB> &h) {
+            uint32_t lo = 0, hi = 0;
+            if (e < H && ch >= h.chunk_base) chunk_span(h.beg, h.deg, 256u, ch - h.chunk_base, &lo, &hi);
+            if (lo >= hi) lo = hi = 0;
+            const uint32_t w0 = lo & ~3u;
+            const uint32_t nc = hi > lo ? (min(256u, E - w0) & ~3u) : 0u;  // whole 16-byte groups inside the array
+            st.src = h.src;
+            st.pay = h.payload;
+            st.lo = lo;
+            st.hi = hi;
+            st.w0 = w0;
+            st.ncopy = nc;
+            dev::fence_proxy_async_smem();
+            dev::mbar_arrive_expect_tx(&st.bar, nc * 4u * (wts ? 2u : 1u));
+            if (nc) {
+                dev::bulk_copy_g2s(st.dst, col + w0, nc * 4u, &st.bar);
+                if (wts) dev::bulk_copy_g2s(st.wt, wts + w0, nc * 4u, &st.bar);
+            }
+        };
+        auto item = [&](uint32_t e) {
+            HeavyItem<TB> h{};
+            if (e < H) h = items[e];
+            return h;
+        };
+        uint32_t e1 = 0xffffffffu, e2 = 0xffffffffu;
+        HeavyItem<TB> h1{};
+        if (lane == 0) {
+            dev::mbar_init(&st.bar, 1);
+            const uint32_t e0 = dev::ld_l2(own + c);
+            issue(c, e0, item(e0));
+            e1 = c + nw < C ? dev::ld_l2(own + c + nw) : 0xffffffffu;
+            h1 = item(e1);
+            e2 = c + 2 * nw < C ? dev::ld_l2(own + c + 2 * nw) : 0xffffffffu;
+        }
+        __syncwarp();
+        uint32_t parity = 0;
+        bool ok = true;
+        for (; c < C; c += nw) {
+            // every lane observes the copy's completion itself; the verdict is warp-uniform
+            ok = __all_sync(dev::kFullMask, dev::mbar_wait_bounded(&st.bar, parity, a.p.timeout_ns));
+            if (!ok) break;
+            parity ^= 1u;
+            __syncwarp();
+            const uint32_t lo = st.lo, hi = st.hi, w0 = st.w0, nc = st.ncopy, src = st.src;
+            const TB pay = st.pay;
+            const uint32_t k0 = lane * 8u;
+            uint32_t d[8], wt[8];
+            if (k0 + 8u <= nc) {
+                const uint4 x = *reinterpret_cast<const uint4 *>(st.dst + k0);
+                const uint4 y = *reinterpret_cast<const uint4 *>(st.dst + k0 + 4);
+                d[0] = x.x, d[1] = x.y, d[2] = x.z, d[3] = x.w, d[4] = y.x, d[5] = y.y, d[6] = y.z, d[7] = y.w;
+                if (wts) {
+                    const uint4 p = *reinterpret_cast<const uint4 *>(st.wt + k0);
+                    const uint4 q = *reinterpret_cast<const uint4 *>(st.wt + k0 + 4);
+                    wt[0] = p.x, wt[1] = p.y, wt[2] = p.z, wt[3] = p.w, wt[4] = q.x, wt[5] = q.y, wt[6] = q.z,
+                    wt[7] = q.w;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) wt[j] = 1u;
+                }
+            } else {  // slots past the staged groups: the array's last (< 4) edges, read directly
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t slot = k0 + j, i = w0 + slot;
+                    const bool in = i >= lo && i < hi;
+                    d[j] = in ? (slot < nc ? st.dst[slot] : __ldg(col + i)) : 0u;
+                    wt[j] = in && wts ? (slot < nc ? st.wt[slot] : __ldg(wts + i)) : 1u;
+                }
+            }
+            __syncwarp();  // the stage is free: the next chunk's copy may overwrite it
+            if (lane == 0 && c + nw < C) {
+                issue(c + nw, e1, h1);
+                e1 = e2;
+                h1 = item(e1);  // arrives while this chunk relaxes
+                e2 = c + 3 * nw < C ? dev::ld_l2(own + c + 3 * nw) : 0xffffffffu;
+            }
+            if (lo < hi) {
+                relax_slots(app, a, s, src, pay, lo, hi, w0 + k0, d, wt, dd, acc);
+                if (lane == 0) acc.edges += hi - lo;
+            }
+        }
+        if (!ok) {
+            // a copy that never completed: report, and give it one more bounded
+            // wait before the stage can be reused or the block exits
+            if (lane == 0) atomicOr(&a.ctrl->cnt.error, dev::kErrTimeout);
+            dev::mbar_wait_bounded(&st.bar, parity, a.p.timeout_ns);
+            return;
+        }
+        __syncwarp();
+        if (lane == 0) dev::mbar_inval(&st.bar);
+        __syncwarp();
     }
 
     static __device__ void clear_dirty(const Args &a, const Snap &s) {

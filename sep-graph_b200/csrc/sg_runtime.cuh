@@ -193,6 +193,7 @@ struct EngineConfig {
     int worklist = 0;          // SG_WORKLIST_* (forced push DD: queues or bitmaps)
     int l2_persist = 0;        // sg_options.l2_persist: >= 0 = persistence window on the random-access array
     int pull_scan = 0;         // sg_options.pull_scan (SG_PULL_SCAN_WARP = warp-cooperative pull)
+    int hub_stage = 0;         // sg_options.hub_stage (>= 0: bulk-copy staging of 256-edge hub chunks)
     bool blocking = true;
     sg_round_trace *trace_out = nullptr;
     uint32_t trace_cap = 0;
@@ -419,6 +420,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     p.sample_cut = cfg.sample_cut;
     p.bitmap_frontier = use_bitmap_frontier(cfg.forced, cfg.lb_push, cfg.wl_sort, cfg.worklist);
     p.pull_coop = cfg.pull_scan == SG_PULL_SCAN_WARP;
+    p.stage_chunks = cfg.hub_stage >= 0;
     p.alpha = cfg.alpha;
     p.beta = cfg.beta;
     p.total_workload0 = (long long)((double)ne * cfg.edge_factor);

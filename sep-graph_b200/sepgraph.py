@@ -58,7 +58,7 @@ class Options(C.Structure):
         ("timeout_s", C.c_double), ("blocking", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("heavy_degree", C.c_int32), ("chunk_edges", C.c_int32), ("team_blocks", C.c_int32),
         ("local_depth", C.c_int32), ("wl_sort", C.c_int32), ("worklist", C.c_int32),
-        ("l2_persist", C.c_int32), ("pull_scan", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("l2_persist", C.c_int32), ("pull_scan", C.c_int32), ("hub_stage", C.c_int32), ("reserved", C.c_int32 * 1),
     ]
 
 

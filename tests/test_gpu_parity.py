@@ -132,7 +132,9 @@ def test_sssp_rmat(ctx, scale):
                    dict(priority="low_high", priority_delta=8), dict(variant="async_pull_dd"),
                    dict(variant="async_push_dd", worklist=2),
                    dict(variant="async_push_dd", priority="low_high", priority_delta=4, worklist=2, local_depth=16),
-                   dict(variant="async_push_dd", priority="low_high", priority_delta=8, worklist=1, chunk_edges=37)):
+                   dict(variant="async_push_dd", priority="low_high", priority_delta=8, worklist=1, chunk_edges=37),
+                   dict(variant="async_push_dd", priority="low_high", priority_delta=8, hub_stage=-1),
+                   dict(variant="async_push_dd", hub_stage=1, heavy_degree=4)):
             d, st, _ = G.sssp(int(src), max_iteration=100000, **kw)
             assert (d == ref).all(), kw
 
@@ -197,6 +199,21 @@ def test_wl_sort_golden(ctx, path):
     for kw in (dict(variant="async_push_dd"), dict(priority="low_high")):
         d, _, _ = G.sssp(src, wl_sort=1, max_iteration=100000, **kw)
         assert (d == g["sssp"]).all(), kw
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=GIDS)
+def test_staged_hub_chunks_golden(ctx, path):
+    """Hub chunks staged by bulk copies (every vertex above 1 edge is split into
+    256-edge chunks here), weighted and unweighted, against the oracle."""
+    g = _load(path)
+    src = int(g["source"])
+    for weighted in (True, False):
+        G = _graph(ctx, g, weighted=weighted)
+        want = g["sssp"] if weighted else g["bfs"]
+        for kw in (dict(), dict(priority="low_high"), dict(blocks_per_sm=8)):
+            d, _, _ = G.sssp(src, variant="async_push_dd", hub_stage=1, heavy_degree=1, chunk_edges=256,
+                             max_iteration=100000, **kw)
+            assert (d == want).all(), (weighted, kw)
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=GIDS)

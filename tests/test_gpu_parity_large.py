@@ -58,6 +58,10 @@ def test_sssp_rmat21(ctx):
                    dict(variant="async_push_dd", priority="low_high", priority_delta=8, worklist=2,
                         chunk_edges=256),
                    dict(variant="async_push_dd", worklist=2, chunk_edges=1024, heavy_degree=64),
+                   dict(variant="async_push_dd", priority="low_high", priority_delta=8, chunk_edges=256,
+                        hub_stage=1),
+                   dict(variant="async_push_dd", priority="low_high", priority_delta=8, chunk_edges=256,
+                        hub_stage=-1),
                    dict(priority="low_high"), dict()):
             d, st, _ = G.sssp(src, max_iteration=1000000, **kw)
             assert (d == ref).all(), kw
