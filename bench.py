@@ -63,6 +63,8 @@ def args_parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--quick", action="store_true", help="headline line only")
     p.add_argument("--served-queries", type=int, default=2000)
+    p.add_argument("--served-slots", type=int, default=3)
+    p.add_argument("--served-bps", type=int, default=0, help="server blocks per SM per slot (0 = library choice)")
     p.add_argument("--extras", default="per_algo,batched,ingest,served", help="extra sections at N=1 (comma list)")
     p.add_argument("--scale", type=int, default=SCALE)
     p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc", "msbfs", "msbc",
@@ -958,7 +960,7 @@ def served(ctx, cache, a):
 
     def stream(qs, rate, seed, **cfg):
         """Submits qs with Poisson arrivals at `rate` queries/s; returns statuses, wall seconds, server stats."""
-        srv = sg.Server(0, slots=3, max_batch=256, **cfg)
+        srv = sg.Server(0, **dict(dict(slots=a.served_slots, max_batch=256, blocks_per_sm=a.served_bps), **cfg))
         try:
             for _, _, gg in graphs:
                 srv.add_graph(gg)

@@ -323,7 +323,9 @@ typedef struct sg_server_config {
                                   max_wait_ms, whose group then goes first; SG_ORDER_OLDEST_FIRST: the
                                   oldest query's group.  Mixed batches always start from the oldest query. */
     uint32_t max_wait_ms;      /* aging bound of SG_ORDER_SHORTEST_FIRST (0 = 500 ms) */
-    int32_t reserved[5];
+    uint32_t blocks_per_sm;    /* resident blocks per SM of each slot's launches (0 = 6 / slots, at least 1):
+                                  the slots' launches share the SMs */
+    int32_t reserved[4];
 } sg_server_config;
 #define SG_BATCH_ONE_GRAPH 1
 #define SG_BATCH_MIXED 2

@@ -98,7 +98,7 @@ sg_options server_options(const sg_server_config &c, int algo) {
     sg_options o;
     sg_options_default(&o);
     o.max_iteration = 1000000;
-    o.blocks_per_sm = std::max(1u, 6u / std::max(1u, c.slots));  // slots share the SMs
+    o.blocks_per_sm = c.blocks_per_sm ? c.blocks_per_sm : std::max(1u, 6u / std::max(1u, c.slots));  // slots share the SMs
     if (algo == SG_QUERY_SSSP) {
         // two-level priority (delta-stepping) with the configured delta, or with
         // each graph's own reference heuristic 32*avg_w/avg_deg when it is 0

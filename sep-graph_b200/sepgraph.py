@@ -116,7 +116,8 @@ class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("max_batch", C.c_uint32),
                 ("max_pending", C.c_uint32), ("msbfs_min", C.c_uint32), ("sssp_delta", C.c_uint32),
                 ("pad", C.c_uint32), ("pr_error", C.c_double), ("batch_graphs", C.c_int32),
-                ("order", C.c_int32), ("max_wait_ms", C.c_uint32), ("reserved", C.c_int32 * 5)]
+                ("order", C.c_int32), ("max_wait_ms", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class Query(C.Structure):
