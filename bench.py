@@ -63,7 +63,7 @@ def args_parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--quick", action="store_true", help="headline line only")
     p.add_argument("--served-queries", type=int, default=2000)
-    p.add_argument("--served-slots", type=int, default=3)
+    p.add_argument("--served-slots", type=int, default=2)
     p.add_argument("--served-bps", type=int, default=0, help="server blocks per SM per slot (0 = library choice)")
     p.add_argument("--extras", default="per_algo,batched,ingest,served", help="extra sections at N=1 (comma list)")
     p.add_argument("--scale", type=int, default=SCALE)
@@ -915,6 +915,7 @@ def served(ctx, cache, a):
     capacity, latency percentiles at 25 / 50 / 90 % of that capacity, and the plain
     one-query-per-launch path on a uniform sample of the stream (results compared)."""
     import sepgraph as sg
+    import torch
 
     specs = [("rmat", sc) for sc in range(14, 23)] + [("grid", n) for n in (1024, 1448, 2048, 2560, 2896, 3584, 4096)]
     graphs = []
@@ -947,13 +948,19 @@ def served(ctx, cache, a):
     # outputs: sampled queries get their own arrays (compared below), the rest share per-graph sinks
     sinks = {}
 
+    def pinned(n, dt):
+        # result arrays in page-locked host memory, as a serving client keeps
+        # them: device-to-host copies run at DMA speed (pageable copies are
+        # staged through the driver and cost about 15 % of the served rate)
+        return torch.zeros(n, dtype=torch.int32).pin_memory().numpy().view(dt)
+
     def out_for(i, algo, gid):
         dt = np.float32 if algo in ("pagerank", "bc") else np.uint32
         if i in sample:
-            return np.zeros(graphs[gid][1].nv, dt)
+            return pinned(graphs[gid][1].nv, dt)
         key = (gid, dt)
         if key not in sinks:
-            sinks[key] = np.zeros(graphs[gid][1].nv, dt)
+            sinks[key] = pinned(graphs[gid][1].nv, dt)
         return sinks[key]
 
     outs = [out_for(i, al, g) for i, (al, g, _) in enumerate(queries)]
@@ -1000,19 +1007,24 @@ def served(ctx, cache, a):
     # plain path: the sampled queries one at a time, results to host like the server's
     plain_lat, same, plain_failed, failed_plain = [], True, 0, set()
     mismatched, pr_l1_max = [], 0.0
+    plain_out = {}  # pinned result arrays, as the served queries have
     for i in sorted(sample):
         al, g, s = queries[i]
         gg = graphs[g][2]
+        key = (g, np.float32 if al in ("pagerank", "bc") else np.uint32)
+        if key not in plain_out:
+            plain_out[key] = pinned(graphs[g][1].nv, key[1])
+        po = plain_out[key]
         t0 = time.perf_counter()
         try:
             if al == "bfs":
-                o, _, _ = gg.bfs(s, max_iteration=1000000)
+                o, _, _ = gg.bfs(s, out=po, max_iteration=1000000)
             elif al == "sssp":
-                o, _, _ = gg.sssp(s, priority="low_high", max_iteration=1000000)
+                o, _, _ = gg.sssp(s, out=po, priority="low_high", max_iteration=1000000)
             elif al == "pagerank":
-                o, _, _ = gg.pagerank(pr_error=1e-7, max_iteration=100000)
+                o, _, _ = gg.pagerank(out=po, pr_error=1e-7, max_iteration=100000)
             else:
-                o, _, _ = gg.bc(s, max_iteration=1000000)
+                o, _, _ = gg.bc(s, out=po, max_iteration=1000000)
         except sg.SGError:
             plain_failed += 1
             failed_plain.add(i)
@@ -1050,6 +1062,7 @@ def served(ctx, cache, a):
         "served_qps": served_qps, "server_qps_first_to_last": st["qps"], "p50_ms": st["p50_ms"],
         "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "batches": st["batches"],
         "load_points": loads, "batch_graphs": "mixed-graph batches from the oldest query (default)",
+        "slots": a.served_slots, "outputs": "pinned host arrays, served and plain alike",
         "one_graph_shortest_first_qps": nq / wall_one,
         "policies": "default: mixed-graph batches from the oldest query; compared: one graph per batch, "
                     "shortest measured (algorithm, graph) group first with a 500 ms aging bound",

@@ -304,7 +304,9 @@ typedef struct sg_server sg_server;
 enum { SG_QUERY_BFS = 0, SG_QUERY_SSSP = 1, SG_QUERY_PAGERANK = 2, SG_QUERY_BC = 3 };
 typedef struct sg_server_config {
     uint64_t hbm_budget_bytes; /* admission budget for batch scratch and staging (0 = 1/4 of HBM) */
-    uint32_t slots;            /* concurrent batches (default 3) */
+    uint32_t slots;            /* concurrent batches (default 2; measured on B200 over the mixed
+                                  16-graph stream: 1 slot 274-280, 2 slots 234-261, 3 slots 174-203
+                                  queries/s, with 2 keeping a long batch from holding up the rest) */
     uint32_t max_batch;        /* queries per batch (default 256) */
     uint32_t max_pending;      /* submit returns SG_ERR_BUSY beyond this (default 1<<20) */
     uint32_t msbfs_min;        /* BFS queries of one graph that go to multi-source BFS (default 4) */
@@ -323,8 +325,9 @@ typedef struct sg_server_config {
                                   max_wait_ms, whose group then goes first; SG_ORDER_OLDEST_FIRST: the
                                   oldest query's group.  Mixed batches always start from the oldest query. */
     uint32_t max_wait_ms;      /* aging bound of SG_ORDER_SHORTEST_FIRST (0 = 500 ms) */
-    uint32_t blocks_per_sm;    /* resident blocks per SM of each slot's launches (0 = 6 / slots, at least 1):
-                                  the slots' launches share the SMs */
+    uint32_t blocks_per_sm;    /* resident blocks per SM of each slot's launches (0 = 6 / slots, at least 1),
+                                  at most 1/slots of what the launched kernel fits per SM, so that every
+                                  slot's cooperative grid is resident beside the others' */
     int32_t reserved[4];
 } sg_server_config;
 #define SG_BATCH_ONE_GRAPH 1

@@ -389,7 +389,7 @@ extern "C" {
 sg_status sg_server_config_default(sg_server_config *c) {
     if (!c) return SG_ERR_INVALID_ARG;
     std::memset(c, 0, sizeof *c);
-    c->slots = 3;
+    c->slots = 2;
     c->max_batch = 256;
     c->max_pending = 1u << 20;
     c->msbfs_min = 4;
@@ -419,6 +419,9 @@ sg_status sg_server_create(int device, const sg_server_config *cfg, sg_server **
             for (auto *x : s->slot_ctx) sg_destroy(x);
             return st;
         }
+        // every slot's persistent grid fits beside the other slots' (a grid
+        // that does not fit would wait for another slot's launch to end)
+        sgb::set_resident_share(c, s->cfg.slots);
         s->slot_ctx.push_back(c);
     }
     uint64_t hbm = 0;

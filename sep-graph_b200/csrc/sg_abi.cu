@@ -245,8 +245,9 @@ sg_status sg_destroy(sg_ctx *ctx) {
     sgb::persist_release(ctx);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->spare_arena) cudaFree(ctx->spare_arena);
-    delete ctx->batch_ws;
+    delete ctx->batch_ws;  // frees on the context's stream and waits for it
     delete ctx->graph_ws;
+    if (cudaMemPool_t pool = sgb::device_pool(ctx->device)) cudaMemPoolTrimTo(pool, 0);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -256,6 +257,9 @@ sg_status sg_destroy(sg_ctx *ctx) {
 
 sg_status sg_ctx_set_stream(sg_ctx *ctx, void *s) {
     if (!ctx) return SG_ERR_INVALID_ARG;
+    // the context's scratch is freed and reused in the order of its stream:
+    // work queued on the old stream ends before the new one can reuse it
+    cudaStreamSynchronize(ctx->stream);
     ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
     return SG_OK;
 }
@@ -447,6 +451,10 @@ sg_status sg_ctx_release_cached(sg_ctx *ctx) {
 
 sg_ctx *sgb::graph_context(const sg_graph *g) { return g ? g->ctx : nullptr; }
 double sgb::graph_weight_sum(const sg_graph *g) { return g ? g->weight_sum : 0.0; }
+
+void sgb::set_resident_share(sg_ctx *ctx, uint32_t share) {
+    if (ctx) ctx->resident_share = std::max(1u, share);
+}
 
 sg_graph *sgb::graph_view(sg_graph *g, sg_ctx *ctx) {
     if (!g || !ctx || g->ctx->device != ctx->device) return nullptr;
@@ -670,7 +678,7 @@ sg_status sg_bc(sg_graph *g, uint32_t source, const sg_options *opt, float *bc_o
         static std::atomic<int> occupancy{0};
         int bps = 0;
         SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, (const void *)bc_backward_kernel, 256, &bps));
-        dim3 grid(ctx->prop.multiProcessorCount * std::max(1, bps));
+        dim3 grid(ctx->prop.multiProcessorCount * sgb::resident_blocks_per_sm(ctx, bps));
         void *args[] = {&ba};
         SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
         SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)bc_backward_kernel, grid, dim3(256), args, 0, ctx->stream));

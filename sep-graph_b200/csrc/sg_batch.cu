@@ -370,7 +370,7 @@ sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint3
     if (row_outs)
         for (uint32_t i = 0; i < nsrc; ++i)
             if (!row_outs[i]) return SG_ERR_INVALID_ARG;
-    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace;
+    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace(&ctx->stream, sgb::device_pool(ctx->device));
     for (uint32_t i = 0; i < nsrc; ++i)
         if (sources[i] >= g->nv) return sgb::set_error(ctx, SG_ERR_INVALID_ARG, "source %u out of range", sources[i]);
     int prev = -1;
@@ -433,7 +433,7 @@ sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint3
     int bps = 0;
     SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, (const void *)msbfs_kernel, kMsThreads, &bps));
     const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::ms_blocks_per_sm(nv, g->ne);
-    dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(bps, want)));
+    dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(sgb::resident_blocks_per_sm(ctx, bps), want)));
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     void *args[] = {&a};
@@ -677,7 +677,8 @@ sg_status prepare_batch(sg_ctx *ctx, sgb::Workspace &ws, std::vector<engine::Bat
     static std::atomic<int> occupancy{0};  // one per template instantiation
     int max_bps = 0;
     SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, B.kernel, kBlockThreads, &max_bps));
-    const int bps = std::max(1, std::min(max_bps, o.blocks_per_sm > 0 ? o.blocks_per_sm : 4));
+    const int bps =
+        std::max(1, std::min(sgb::resident_blocks_per_sm(ctx, max_bps), o.blocks_per_sm > 0 ? o.blocks_per_sm : 4));
     const uint32_t total_blocks = (uint32_t)(ctx->prop.multiProcessorCount * bps);
     // Automatic team size.  Equal teams claim queries largest first, so the
     // batch lasts at least as long as its largest query on one team: a team
@@ -916,7 +917,7 @@ template <typename App, typename TV, typename TB, typename TW>
 sg_status run_batch(sg_ctx *ctx, std::vector<engine::BatchQuery<App, TV>> qs, const std::vector<sg_graph *> &graphs,
                     const std::vector<void *> &outs, const sg_options &o, engine::Params p, sg_stats *stats,
                     float *per_query_ms) {
-    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace;
+    if (!ctx->batch_ws) ctx->batch_ws = new sgb::Workspace(&ctx->stream, sgb::device_pool(ctx->device));
     BatchBuild B;
     sg_status st = prepare_batch<App, TV, TB, TW>(ctx, *ctx->batch_ws, std::move(qs), graphs, outs, o, p, false, B);
     if (st != SG_OK) return st;

@@ -63,7 +63,7 @@ struct Tmp {
     cudaError_t alloc(T **p, uint64_t count) {
         char name[48];
         std::snprintf(name, sizeof name, "gb_%s_%u", prefix, n++);
-        if (!ctx->graph_ws) ctx->graph_ws = new Workspace;
+        if (!ctx->graph_ws) ctx->graph_ws = new Workspace(&ctx->stream, device_pool(ctx->device));
         return ctx->graph_ws->get(name, (size_t)std::max<uint64_t>(count, 1), p);
     }
 };

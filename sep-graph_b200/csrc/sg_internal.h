@@ -27,6 +27,10 @@ double graph_weight_sum(const sg_graph *g);
 // before g is destroyed.
 sg_graph *graph_view(sg_graph *g, sg_ctx *ctx);
 void graph_view_destroy(sg_graph *view);
+// Number of contexts (ctx among them) whose persistent launches run side by
+// side; each launch on ctx then takes at most that share of a kernel's
+// resident blocks per SM (1, the default, lets a launch fill the device).
+void set_resident_share(sg_ctx *ctx, uint32_t share);
 
 // Device graph from a CSR (host or device arrays): one upload, validation on
 // the device, and the in-edge (CSC) view from the device transpose.

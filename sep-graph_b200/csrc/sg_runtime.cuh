@@ -43,6 +43,11 @@ struct sg_ctx {
     void *spare_arena = nullptr;
     size_t spare_bytes = 0;
     bool persist_ref = false;  // holds a reference on the device's persisting-L2 set-aside
+    // Contexts whose persistent launches run side by side on the device (a
+    // server's slots): each launch takes at most 1/resident_share of a kernel's
+    // resident blocks per SM, so that every slot's cooperative grid fits beside
+    // the others' instead of waiting for one of them to end.
+    uint32_t resident_share = 1;
 };
 
 namespace sgb {
@@ -52,13 +57,54 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
-// Grow-only device buffers owned by one graph.  Work on a context is ordered
-// on its stream, so consecutive queries reuse them without reallocating.
+// Stream-ordered memory pool of a device, created on first use, that keeps
+// freed memory for reuse (release threshold at its maximum) until a context is
+// destroyed (sg_destroy trims it).  nullptr when the device offers no pool.
+inline cudaMemPool_t device_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = p;
+    }
+    return pools[device];
+}
+
+// Grow-only device buffers owned by one context.  Work on a context is ordered
+// on its stream, so consecutive queries reuse them without reallocating.  A
+// context's workspaces allocate, zero and free on the context's stream from
+// the device pool: growing a buffer never waits for work that other contexts
+// (a server's other slots) have in flight, as cudaFree would.  A workspace
+// without a stream (a batch plan's, whose addresses a captured graph holds)
+// uses cudaMalloc and cudaFree.
 struct Workspace {
     std::map<std::string, DevBuf> bufs;
+    const cudaStream_t *stream = nullptr;  // the owning context's current stream
+    cudaMemPool_t pool = nullptr;
+    Workspace() = default;
+    Workspace(const cudaStream_t *s, cudaMemPool_t p) : stream(s), pool(p) {}
+    Workspace(const Workspace &) = delete;
+    Workspace &operator=(const Workspace &) = delete;
+    bool ordered() const { return stream && pool; }
     ~Workspace() {
         for (auto &kv : bufs)
-            if (kv.second.p) cudaFree(kv.second.p);
+            if (kv.second.p) {
+                if (ordered()) cudaFreeAsync(kv.second.p, *stream);
+                else cudaFree(kv.second.p);
+            }
+        if (ordered()) cudaStreamSynchronize(*stream);
     }
     template <typename T>
     cudaError_t get(const char *name, size_t count, T **out, bool zero_new = false) {
@@ -67,14 +113,17 @@ struct Workspace {
         if (bytes == 0) bytes = 256;
         bytes = (bytes + 255) & ~size_t(255);
         if (b.bytes < bytes) {
-            if (b.p) cudaFree(b.p);
+            if (b.p) {
+                if (ordered()) cudaFreeAsync(b.p, *stream);
+                else cudaFree(b.p);
+            }
             b.p = nullptr;
             b.bytes = 0;
-            cudaError_t e = cudaMalloc(&b.p, bytes);
+            cudaError_t e = ordered() ? cudaMallocFromPoolAsync(&b.p, bytes, pool, *stream) : cudaMalloc(&b.p, bytes);
             if (e != cudaSuccess) return e;
             b.bytes = bytes;
             if (zero_new) {
-                e = cudaMemset(b.p, 0, bytes);
+                e = ordered() ? cudaMemsetAsync(b.p, 0, bytes, *stream) : cudaMemset(b.p, 0, bytes);
                 if (e != cudaSuccess) return e;
             }
         }
@@ -107,7 +156,7 @@ namespace sgb {
 // all its graphs (work of a context is ordered on its stream), so creating
 // another graph allocates no new scratch.
 inline Workspace &graph_ws(sg_graph *g) {
-    if (!g->ctx->graph_ws) g->ctx->graph_ws = new Workspace;
+    if (!g->ctx->graph_ws) g->ctx->graph_ws = new Workspace(&g->ctx->stream, device_pool(g->ctx->device));
     return *g->ctx->graph_ws;
 }
 }  // namespace sgb
@@ -309,6 +358,14 @@ inline cudaError_t occupancy_once(std::atomic<int> &cache, const void *kernel, i
     return cudaSuccess;
 }
 
+// Blocks per SM a launch on ctx may take of a kernel that fits max_bps per SM:
+// max_bps / ctx->resident_share (at least 1).  Any set of launches from
+// resident_share such contexts then needs at most the SM's registers, shared
+// memory and threads, so their grids are resident together.
+inline int resident_blocks_per_sm(const sg_ctx *ctx, int max_bps) {
+    return std::max(1, max_bps / (int)std::max(1u, ctx->resident_share));
+}
+
 // Resident blocks per SM of the multi-source kernels (BFS masks, BC lanes)
 // when the caller does not choose: sparse high-diameter graphs are bound by
 // the per-level barrier (fewer blocks), large dense ones by memory latency
@@ -441,7 +498,7 @@ sg_status run_engine(sg_graph *g, App app, const EngineConfig &cfg, TV *value, T
     SG_TRY_CUDA(ctx, occupancy_once(occupancy, (const void *)kernel, kBlockThreads, &max_blocks_per_sm));
     if (max_blocks_per_sm <= 0) return set_error(ctx, SG_ERR_NO_DEVICE, "engine kernel cannot be resident");
     int bps = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : auto_blocks_per_sm(nv, ne);
-    bps = std::max(1, std::min(bps, max_blocks_per_sm));
+    bps = std::max(1, std::min(bps, resident_blocks_per_sm(ctx, max_blocks_per_sm)));
     dim3 grid(ctx->prop.multiProcessorCount * bps), block(kBlockThreads);
     res->grid_blocks = grid.x;
     if (cfg.wl_sort) SG_TRY_CUDA(ctx, ws.get("sort", grid.x, &a.sort_counts));
