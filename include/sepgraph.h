@@ -325,7 +325,8 @@ typedef struct sg_server_config {
                                   max_wait_ms, whose group then goes first; SG_ORDER_OLDEST_FIRST: the
                                   oldest query's group.  Mixed batches always start from the oldest query. */
     uint32_t max_wait_ms;      /* aging bound of SG_ORDER_SHORTEST_FIRST (0 = 500 ms) */
-    uint32_t blocks_per_sm;    /* resident blocks per SM of each slot's launches (0 = 6 / slots, at least 1),
+    uint32_t blocks_per_sm;    /* resident blocks per SM of each slot's launches (0 = 6 / slots, at least 1,
+                                  for team batches; multi-source BFS / BC choose by graph and source count),
                                   at most 1/slots of what the launched kernel fits per SM, so that every
                                   slot's cooperative grid is resident beside the others' */
     int32_t reserved[4];

@@ -183,6 +183,8 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
                 continue;
             }
             const GraphInfo &gi = graphs[kv.first];
+            sg_options om = o;  // multi-source launches size their own grid unless the config fixes it
+            om.blocks_per_sm = (int32_t)cfg.blocks_per_sm;
             for (size_t s = 0; s < kv.second.size(); s += 64) {
                 const size_t m = std::min<size_t>(64, kv.second.size() - s);
                 std::vector<uint32_t> src(m);
@@ -191,7 +193,7 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
                     src[k] = b[kv.second[s + k]].q.source;
                     rows[k] = (uint32_t *)b[kv.second[s + k]].q.out;  // each level row straight to its query
                 }
-                const sg_status st = sgb::msbfs_on(ctx, gi.g, src.data(), (uint32_t)m, &o, nullptr, nullptr, rows.data());
+                const sg_status st = sgb::msbfs_on(ctx, gi.g, src.data(), (uint32_t)m, &om, nullptr, nullptr, rows.data());
                 for (size_t k = 0; k < m; ++k) status[kv.second[s + k]] = st;
             }
         }
@@ -258,7 +260,9 @@ void sg_server::run_batch(int slot, std::vector<Pending> &b, std::vector<sg_stat
                         src[k] = b[kv.second[s + k]].q.source;
                         rows[k] = (float *)b[kv.second[s + k]].q.out;
                     }
-                    ok = sgb::msbc_rows(gv, src.data(), (uint32_t)m, &o, nullptr, rows.data(), nullptr) == SG_OK;
+                    sg_options om = o;  // the multi-source launch sizes its own grid unless the config fixes it
+                    om.blocks_per_sm = (int32_t)cfg.blocks_per_sm;
+                    ok = sgb::msbc_rows(gv, src.data(), (uint32_t)m, &om, nullptr, rows.data(), nullptr) == SG_OK;
                 }
                 if (ok) continue;
                 for (size_t k = 0; k < m; ++k) {

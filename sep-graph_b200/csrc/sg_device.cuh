@@ -187,6 +187,34 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *queue, uint32_t *count
     return m;
 }
 
+// Appends, for every lane, items[k] for each set bit k (< 4) of `which`, with
+// one atomic per warp on `count`; all 32 lanes must call it.
+__device__ __forceinline__ void warp_append4(uint32_t *queue, uint32_t *count, uint32_t cap, uint32_t which,
+                                             const uint32_t (&items)[4], uint32_t *err) {
+    const uint32_t c = __popc(which);
+    uint32_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFullMask, incl, d);
+        if (lane_id() >= (uint32_t)d) incl += y;
+    }
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    if (total == 0) return;
+    uint32_t base = 0;
+    if (lane_id() == 31) base = atomicAdd(count, total);
+    base = __shfl_sync(kFullMask, base, 31);
+    uint32_t pos = base + incl - c;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if ((which >> k) & 1u) {
+            if (pos < cap)
+                queue[pos] = items[k];
+            else
+                atomicOr(err, kErrCapacity);
+            ++pos;
+        }
+}
+
 __device__ __forceinline__ bool bitmap_test(const uint32_t *bm, uint32_t v) {
     return (ld_l2(bm + (v >> 5)) >> (v & 31u)) & 1u;
 }

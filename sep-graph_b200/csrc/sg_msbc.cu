@@ -464,7 +464,7 @@ sg_status msbc_rows(sg_graph *g, const uint32_t *sources, uint32_t nsrc, const s
     int bps = 0;
     SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, (const void *)msbc_kernel, kMbThreads, &bps));
     if (bps <= 0) return sgb::set_error(ctx, SG_ERR_NO_DEVICE, "multi-source BC kernel cannot be resident");
-    const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::ms_blocks_per_sm(nv, g->ne);
+    const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::ms_blocks_per_sm(nv, g->ne, nsrc);
     const dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(sgb::resident_blocks_per_sm(ctx, bps), want)));
     // a vertex appears once per depth at which some source reaches it; start
     // with 8 depths per vertex and retry with the bound of 32
