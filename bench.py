@@ -68,7 +68,7 @@ def args_parse():
     p.add_argument("--extras", default="per_algo,batched,ingest,served", help="extra sections at N=1 (comma list)")
     p.add_argument("--scale", type=int, default=SCALE)
     p.add_argument("--profile", choices=["sssp_push", "sssp_delta", "bfs", "pr_pull", "pr_push", "bc", "msbfs", "msbc",
-                                         "sssp_batch", "transpose"],
+                                         "msbfs_grid", "sssp_batch", "transpose"],
                    help="run one warm-up and one measured solve of that kernel only (for ncu captures)")
     p.add_argument("--opts", default="", help="--profile: JSON object of sg_options fields overriding the mode's")
     return p.parse_args()
@@ -79,7 +79,7 @@ def run_profile(a):
     import sepgraph as sg
 
     ctx = sg.Context(int(os.environ.get("LOCAL_RANK", "0")))
-    if a.profile in ("msbfs", "msbc", "sssp_batch", "transpose"):
+    if a.profile in ("msbfs", "msbc", "msbfs_grid", "sssp_batch", "transpose"):
         run_profile_batch(a, ctx)
         ctx.close()
         return
@@ -113,7 +113,8 @@ def run_profile(a):
 
 def run_profile_batch(a, ctx):
     """Two runs of one batched / multi-source / graph-construction call (the second is the one to capture):
-    msbfs 64 sources and msbc 32 sources on the symmetric RMAT graph of --scale; sssp_batch 64 SSSP
+    msbfs 64 sources and msbc 32 sources on the symmetric RMAT graph of --scale; msbfs_grid 64 sources
+    on the 2^(scale/2) x 2^(scale/2) 4-neighbour grid (interleaved masks); sssp_batch 64 SSSP
     queries over RMAT graphs of scales 12 .. --scale; transpose = sg_graph_create of the directed
     weighted RMAT CSR of --scale from device arrays (validation and the CSC transpose)."""
     import sepgraph as sg
@@ -129,6 +130,13 @@ def run_profile_batch(a, ctx):
             srcs = [int(x) for x in h.pick_sources(n, 11)]
             out = G.msbfs(srcs) if a.profile == "msbfs" else G.msbc(srcs)
             ms = out[1].time_kernel_ms
+        elif a.profile == "msbfs_grid":
+            if _ == 0:
+                side = 1 << (a.scale // 2)
+                h = sg.HostGraph.grid(side, side)
+                G = ctx.graph(h)
+                srcs = [int(x) for x in np.random.default_rng(5).integers(0, h.nv, 64)]
+            ms = G.msbfs(srcs, max_iteration=1000000)[1].time_kernel_ms
         elif a.profile == "sssp_batch":
             if _ == 0:
                 graphs = []
