@@ -1075,7 +1075,7 @@ def served(ctx, cache, a):
         "policies": "default: mixed-graph batches from the oldest query; compared: one graph per batch, "
                     "shortest measured (algorithm, graph) group first with a 500 ms aging bound",
         "failed": failed, "plain_failed": plain_failed, "hbm_peak_bytes": st["hbm_peak"],
-        "hbm_budget_bytes": st["hbm_budget"], "sssp": "two-level priority, each graph's delta heuristic",
+        "hbm_budget_bytes": st["hbm_budget"], "sssp": "delta-stepping (push, two-level priority, lookahead 4), each graph's delta heuristic",
         "plain_sample": len(plain_lat), "plain_qps": plain_qps, "plain_p50_ms": pct(plain_lat_sorted, 0.5),
         "plain_p99_ms": pct(plain_lat_sorted, 0.99), "speedup_qps": served_qps / plain_qps,
         "sample_results_same": same, "mismatched": mismatched, "pagerank_l1_max": pr_l1_max,
