@@ -1028,7 +1028,9 @@ def served(ctx, cache, a):
             if al == "bfs":
                 o, _, _ = gg.bfs(s, out=po, max_iteration=1000000)
             elif al == "sssp":
-                o, _, _ = gg.sssp(s, out=po, priority="low_high", max_iteration=1000000)
+                # the server's SSSP method (delta-stepping push, lookahead 4), one query per launch
+                o, _, _ = gg.sssp(s, out=po, variant="async_push_dd", priority="low_high", local_depth=4,
+                                  max_iteration=1000000)
             elif al == "pagerank":
                 o, _, _ = gg.pagerank(out=po, pr_error=1e-7, max_iteration=100000)
             else:
@@ -1081,7 +1083,8 @@ def served(ctx, cache, a):
         "sample_results_same": same, "mismatched": mismatched, "pagerank_l1_max": pr_l1_max,
         "plain_ms_by_algo": {k: {"queries": c, "mean_ms": t / c} for k, (c, t) in by_algo.items()},
         "note": "plain path = one blocking call per query on the sampled 1-in-10 queries, service time only "
-                "(no queueing); served latency includes queueing under the offered Poisson load",
+                "(no queueing), each algorithm with the server's method (SSSP: delta-stepping push, "
+                "lookahead 4); served latency includes queueing under the offered Poisson load",
     }
 
 
