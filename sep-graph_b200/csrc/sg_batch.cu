@@ -396,6 +396,156 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
     }
 }
 
+// Push-only multi-source BFS with one barrier per round, for sparse graphs
+// (average degree below 8: grids, road networks), where push rounds are the
+// only ones that pay and hubs are absent.  The vertices discovered in round k
+// (list T[p], their new bits pending in next[p]) are settled in round k + 1
+// by the thread that expands them: it fixes their seen mask and levels and
+// ORs their new bits straight into their neighbours' next[p ^ 1], so the
+// two-phase kernel's separate settle pass and its barrier disappear.  A
+// neighbour's seen mask read while another thread settles that neighbour may
+// miss the bits being settled; the OR then carries bits the neighbour already
+// has, which its own settle drops (nb = next & ~seen), so levels are exact.
+// Each vertex enters T[p ^ 1] at most once a round (the OR that found its
+// next[p ^ 1] zero lists it), and its settle zeroes next[p] again.  Masks:
+// fields kSeen, kNext0 + p (the record's third word is next[1]).  Round
+// state: qin = p, F = |T[p]|, pile = 1 for the settle-only round that ends a
+// launch at max_rounds.
+__global__ void __launch_bounds__(kMsThreads) msbfs_fused_kernel(MsArgs a) {
+    Ctrl *c = a.ctrl;
+    engine::set_team(blockIdx.x, gridDim.x, c);
+    __shared__ engine::RoundState s;
+    engine::Counters *n = &c->cnt;
+    const uint32_t lane = dev::lane_id();
+    const uint32_t gw = gthread() >> 5, nw = nthreads() >> 5;
+    engine::PolicyState ps;  // leader's round state (block 0, thread 0)
+    auto nop = [] {};
+
+    for (uint32_t v = gthread(); v < a.nv; v += nthreads()) {
+        for (uint32_t f = 0; f < 4; ++f) *a.m.at(f, v) = 0;
+    }
+    const uint64_t total_lv = (uint64_t)a.nsrc * a.nv;
+    for (uint64_t k = gthread(); k < total_lv; k += nthreads()) a.levels[k] = 0xffffffffu;
+    if (!engine::grid_sync(c, a.timeout_ns, nop)) return;
+    if (gthread() < a.nsrc) {  // the sources' bits pending in next[0], each vertex listed once in T[0]
+        const uint32_t v = a.sources[gthread()];
+        const unsigned long long old = atomicOr(a.m.at(kNext, v), 1ull << gthread());
+        if (old == 0) a.active[0][atomicAdd(&n->qcount[0], 1u)] = v;
+    }
+    auto start = [&] {
+        memset(&ps, 0, sizeof ps);
+        ps.rs.round = 0;
+        ps.rs.qin = 0;
+        ps.rs.F = dev::ld_l2(&n->qcount[0]);
+        ps.rs.pile = a.max_rounds == 0 ? 1u : 0u;
+        const uint4 *src = reinterpret_cast<const uint4 *>(&ps.rs);
+        for (int k = 0; k < 4; ++k) __stcg(reinterpret_cast<uint4 *>(&c->rs) + k, src[k]);
+    };
+    if (!engine::grid_sync(c, a.timeout_ns, start)) return;
+
+    uint32_t u4[4];
+    for (;;) {
+        if (threadIdx.x < 4)
+            reinterpret_cast<uint4 *>(&s)[threadIdx.x] = __ldcg(reinterpret_cast<const uint4 *>(&c->rs) + threadIdx.x);
+        __syncthreads();
+        if (s.done) break;
+        const uint32_t p = s.qin, q = p ^ 1u;
+        const bool expand = s.pile == 0;
+        const uint32_t *T = a.active[p];
+        unsigned long long edges = 0;
+        // OR f into up to four neighbours col[e + k * stride] (e + k * stride < end)
+        // of next[q]; returns the bits k whose OR was that vertex's first (it is
+        // listed in T[q])
+        auto push4 = [&](uint32_t e, uint32_t end, uint32_t stride, unsigned long long f) {
+            unsigned long long sn[4], nx[4], old[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                u4[k] = (uint64_t)e + k * stride < end ? __ldg(a.col + e + k * stride) : kNoVertex;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                sn[k] = nx[k] = ~0ull;
+                if (u4[k] != kNoVertex) {
+                    sn[k] = __ldcg(a.m.at(kSeen, u4[k]));
+                    nx[k] = __ldcg(a.m.at(kNext + q, u4[k]));
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const unsigned long long add = f & ~sn[k];
+                old[k] = add && (nx[k] & add) != add ? atomicOr(a.m.at(kNext + q, u4[k]), add) : 1ull;
+            }
+            uint32_t first = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) first |= (old[k] == 0 ? 1u : 0u) << k;
+            return first;
+        };
+        for (uint32_t base = gw * 32; base < s.F; base += nw * 32) {
+            const uint32_t i = base + lane;
+            uint32_t u = 0, beg = 0, deg = 0;
+            unsigned long long nb = 0;
+            if (i < s.F) {
+                u = __ldcg(T + i);
+                const unsigned long long was = __ldcg(a.m.at(kSeen, u));
+                const unsigned long long nx = __ldcg(a.m.at(kNext + p, u));
+                nb = nx & ~was;
+                *a.m.at(kNext + p, u) = 0;
+                if (nb) {
+                    *a.m.at(kSeen, u) = was | nb;
+                    for (unsigned long long m = nb; m; m &= m - 1)
+                        a.levels[(uint64_t)(__ffsll(m) - 1) * a.nv + u] = s.round;
+                    if (expand) {
+                        beg = __ldg(a.row + u);
+                        deg = __ldg(a.row + u + 1) - beg;
+                    }
+                }
+            }
+            // a thread per vertex up to kMsWarp edges, four per step (all lanes step together)
+            const bool mid = deg > kMsWarp;
+            const uint32_t mine = mid ? 0u : deg;
+            const uint32_t steps = __reduce_max_sync(dev::kFullMask, (mine + 3u) >> 2);
+            for (uint32_t st = 0; st < steps; ++st) {
+                const uint32_t first = push4(beg + 4 * st, beg + mine, 1, nb);
+                dev::warp_append4(a.active[q], &n->qcount[q], a.nv, first, u4, &n->error);
+            }
+            edges += mine;
+            // larger lists: a whole warp per vertex
+            uint32_t m = __ballot_sync(dev::kFullMask, mid);
+            while (m) {
+                const uint32_t j = __ffs(m) - 1;
+                m &= m - 1;
+                const uint32_t bj = __shfl_sync(dev::kFullMask, beg, j), dj = __shfl_sync(dev::kFullMask, deg, j);
+                const unsigned long long fj = __shfl_sync(dev::kFullMask, nb, j);
+                for (uint32_t off = 0; off < dj; off += 128) {
+                    const uint32_t first = push4(bj + off + lane, bj + dj, 32, fj);
+                    dev::warp_append4(a.active[q], &n->qcount[q], a.nv, first, u4, &n->error);
+                }
+                if (lane == 0) edges += dj;
+            }
+        }
+        edges = dev::warp_sum(edges);
+        if (lane == 0 && edges) atomicAdd(&n->edges_processed, edges);
+        auto end_round = [&] {
+            const uint32_t F2 = dev::ld_l2(&n->qcount[q]);
+            const uint32_t F_in = ps.rs.F;
+            n->qcount[p] = 0;
+            const bool settle_only = ps.rs.pile != 0;
+            ps.rs.qin = q;
+            ps.rs.F = F2;
+            ps.rs.round++;
+            ps.rs.pile = ps.rs.round >= a.max_rounds ? 1u : 0u;  // the last round settles without expanding
+            if (F2 == 0 || settle_only) {
+                ps.rs.done = 1;
+                c->round = settle_only ? ps.rs.round - 1 : ps.rs.round;  // expanding rounds
+                c->rounds_by_variant[engine::V_ASYNC_PUSH_DD] = c->round;
+                c->max_iteration_reached = settle_only && F_in != 0;
+            }
+            const uint4 *src = reinterpret_cast<const uint4 *>(&ps.rs);
+            for (int k = 0; k < 4; ++k) __stcg(reinterpret_cast<uint4 *>(&c->rs) + k, src[k]);
+        };
+        if (!engine::grid_sync(c, a.timeout_ns, end_round)) return;
+    }
+}
+
 // Edges of the reached component summed over sources: sum_v popcount(seen[v]) * deg(v).
 __global__ void msbfs_reach_kernel(const uint32_t *row, MsMasks m, uint32_t nv, unsigned long long *out) {
     unsigned long long e = 0;
@@ -488,15 +638,19 @@ sg_status sgb::msbfs_on(sg_ctx *ctx, sg_graph *g, const uint32_t *sources, uint3
     a.force_dir = o.variant == SG_ASYNC_PUSH_DD ? 0 : (o.variant == SG_ASYNC_PULL_DD ? 1 : -1);
     if (!g->has_csc && !g->symmetric) a.force_dir = 0;
 
-    static std::atomic<int> occupancy{0};
+    // sparse graphs run push-only with one barrier per round (msbfs_fused_kernel)
+    // unless pull is forced; the rest take the two-phase push/pull kernel
+    const bool fused = interleaved && a.force_dir != 1;
+    const void *kernel = fused ? (const void *)msbfs_fused_kernel : (const void *)msbfs_kernel;
+    static std::atomic<int> occupancy[2] = {{0}, {0}};
     int bps = 0;
-    SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy, (const void *)msbfs_kernel, kMsThreads, &bps));
+    SG_TRY_CUDA(ctx, sgb::occupancy_once(occupancy[fused ? 1 : 0], kernel, kMsThreads, &bps));
     const int want = o.blocks_per_sm > 0 ? o.blocks_per_sm : sgb::ms_blocks_per_sm(nv, g->ne, nsrc);
     dim3 grid(ctx->prop.multiProcessorCount * std::max(1, std::min(sgb::resident_blocks_per_sm(ctx, bps), want)));
     SG_TRY_CUDA(ctx, cudaMemsetAsync(a.ctrl, 0, sizeof(Ctrl), ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     void *args[] = {&a};
-    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)msbfs_kernel, grid, dim3(kMsThreads), args, 0, ctx->stream));
+    SG_TRY_CUDA(ctx, cudaLaunchCooperativeKernel(kernel, grid, dim3(kMsThreads), args, 0, ctx->stream));
     SG_TRY_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     if (!o.blocking) return SG_OK;
     Ctrl h;

@@ -60,6 +60,59 @@ def test_msbfs_matches_single_source_engine(ctx):
         assert (lv[i] == single).all()
 
 
+def _csr(nv, src, dst):
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    off = np.zeros(nv + 1, np.uint32)
+    np.add.at(off, src.astype(np.int64) + 1, 1)
+    return np.cumsum(off, dtype=np.uint64).astype(np.uint32), dst.astype(np.uint32)
+
+
+def test_msbfs_sparse_push_only_with_a_hub(ctx):
+    """Sparse graphs (average degree below 8) run the one-barrier push-only
+    kernel; a vertex of 1,500 out-edges there is expanded by a whole warp.
+    Every row equals the oracle; forced pull (two-phase kernel) agrees."""
+    w, hgt = 40, 50
+    nv = w * hgt + 1
+    hub = nv - 1
+    src, dst = [], []
+    for y in range(hgt):
+        for x in range(w):
+            v = y * w + x
+            for dx, dy in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+                if 0 <= x + dx < w and 0 <= y + dy < hgt:
+                    src.append(v)
+                    dst.append((y + dy) * w + x + dx)
+    rng = np.random.default_rng(3)
+    far = rng.choice(nv - 1, 1500, replace=False)
+    src += [hub] * len(far) + [0]
+    dst += list(far) + [hub]
+    off, idx = _csr(nv, np.array(src, np.int64), np.array(dst, np.int64))
+    G = ctx.graph_from_csr(off, idx)
+    srcs = np.array([0, hub, 777, 1999, 0], np.uint32)
+    want = [oracle.bfs(off, idx, int(s)) for s in srcs]
+    for variant in ("auto", "async_push_dd", "async_pull_dd"):
+        lv, st = G.msbfs(srcs, variant=variant, max_iteration=100000)
+        for i in range(len(srcs)):
+            assert (lv[i] == want[i]).all(), (variant, i)
+
+
+@pytest.mark.parametrize("max_iteration", [1, 7, 40])
+def test_msbfs_max_iteration_truncates_alike(ctx, max_iteration):
+    """With a round limit, both kernels settle exactly the levels up to it."""
+    h = sg.HostGraph.grid(64, 80)
+    G = ctx.graph(h)
+    srcs = np.array([0, 5119, 2500, 77], np.uint32)
+    fused, st_f = G.msbfs(srcs, max_iteration=max_iteration)
+    pulled, st_p = G.msbfs(srcs, variant="async_pull_dd", max_iteration=max_iteration)
+    assert (fused == pulled).all()
+    for i, s in enumerate(srcs):
+        full = oracle.bfs(h.offsets, h.indices, int(s))
+        want = np.where(full <= max_iteration, full, full.dtype.type(sg.INF))
+        assert (fused[i] == want).all(), i
+    assert st_f.max_iteration_reached == st_p.max_iteration_reached
+
+
 @pytest.fixture(scope="module")
 def uneven_graphs(ctx):
     """Graphs of uneven size (RMAT scales 8-14, directed and symmetric, a grid), weights in [1,64)."""
