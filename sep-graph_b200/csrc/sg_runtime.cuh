@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -371,13 +372,15 @@ inline int resident_blocks_per_sm(const sg_ctx *ctx, int max_bps) {
 // the per-level barrier (fewer blocks), large dense ones by memory latency
 // (more).  Measured on B200: 16 BFS on the 4096^2 grid 197 / 229 / 288 ms with
 // 2 / 4 / 6 blocks; 64 BFS and 32 BC on symmetric RMAT-22 9.4 -> 8.2 and
-// 23.3 -> 21.1 ms from 4 to 6; RMAT-16 best with 4.  Many sources on a
-// large sparse graph fill more blocks: 64 BFS on the 4096^2 grid 787 / 735 /
-// 683 ms with 2 / 3 / 4 blocks (16 BFS there, or 64 on the 2048^2 grid, no
-// faster than with 2).
+// 23.3 -> 21.1 ms from 4 to 6; RMAT-16 best with 4.  On a sparse graph a
+// round's work grows with the sources times the wavefront (about sqrt(V) on
+// a grid), and a large one fills more blocks: push-only multi-source BFS, 64
+// sources on the 4096^2 grid 1030 / 650 / 521 / 462 ms with 1 / 2 / 3 / 4
+// blocks, on the 2048^2 grid 119 / 80 / 78 / 75 ms; 16 sources there 137 /
+// 126 / 135 / 149 ms and 39 / 42 / 48 / 54 ms.
 inline int ms_blocks_per_sm(uint32_t nv, uint64_t ne, uint32_t nsrc) {
     const double avg_deg = nv ? (double)ne / nv : 0.0;
-    if (avg_deg < 8) return (uint64_t)nsrc * nv >= (1ull << 30) ? 4 : 2;
+    if (avg_deg < 8) return (double)nsrc * std::sqrt((double)nv) >= 131072.0 ? 4 : 2;
     return ne >= (1ull << 25) ? 6 : 4;
 }
 
