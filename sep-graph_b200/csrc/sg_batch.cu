@@ -51,7 +51,9 @@ constexpr uint32_t kNoVertex = 0xffffffffu;  // an empty edge slot (vertex ids a
 //    million vertices stays in L2 (64 BFS on directed RMAT-22 7.7 ms dense,
 //    8.8 ms interleaved).
 // Sparse high-diameter graphs (average degree below 8) run push rounds, so
-// they take the interleaved layout.
+// they take the interleaved layout (the push-only kernel below keeps seen and
+// the two round parities' next masks there; the two-phase kernel, when pull
+// is forced on such a graph, its four masks).
 enum : uint32_t { kSeen = 0, kNext = 1, kFr0 = 2 };
 struct MsMasks {
     unsigned long long *base;
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_kernel(MsArgs a) {
 // has, which its own settle drops (nb = next & ~seen), so levels are exact.
 // Each vertex enters T[p ^ 1] at most once a round (the OR that found its
 // next[p ^ 1] zero lists it), and its settle zeroes next[p] again.  Masks:
-// fields kSeen, kNext0 + p (the record's third word is next[1]).  Round
+// fields kSeen and kNext + p (the record's third word holds next[1]).  Round
 // state: qin = p, F = |T[p]|, pile = 1 for the settle-only round that ends a
 // launch at max_rounds.
 __global__ void __launch_bounds__(kMsThreads) msbfs_fused_kernel(MsArgs a) {
